@@ -1,0 +1,306 @@
+// Test infrastructure only: a project-written subset of the Kokkos programming model that lets the
+// unmodified ExaCA reference sources compile on this host, where Kokkos itself is not installed.
+// It is used to build the oracle (serial dispatch, ascending index order) and the CPU baseline
+// (OpenMP dispatch) under oracle/_ref/. Nothing in the product links or includes it.
+//
+// Only the symbols the reference touches are provided (29 of them; see the grep in the build recipe).
+// Semantics follow the public Kokkos documentation:
+//  - View<T*>, View<T**>, View<T***>: LayoutRight host storage, reference-counted shallow copies.
+//  - ViewAllocateWithoutInitializing: storage is zero-filled here (calloc); the reference relies on
+//    fresh pages being zero for cells a spot-melt temperature init never writes.
+//  - create_mirror_view_and_copy(HostSpace, v) returns v itself (same memory space => no copy).
+//  - resize keeps the overlapping prefix and zero-fills new storage.
+//  - parallel_for / parallel_reduce: ascending index order when EXACA_SHIM_OPENMP is undefined,
+//    an OpenMP static schedule otherwise.
+#ifndef EXACA_ORACLE_KOKKOS_SHIM_HPP
+#define EXACA_ORACLE_KOKKOS_SHIM_HPP
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdlib>
+#include <cstring>
+#include <iostream>
+#include <limits>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <type_traits>
+#include <utility>
+#ifdef EXACA_SHIM_OPENMP
+#include <omp.h>
+#endif
+
+#define KOKKOS_LAMBDA [=]
+#define KOKKOS_INLINE_FUNCTION inline
+#define KOKKOS_FORCEINLINE_FUNCTION inline
+
+namespace Kokkos {
+
+struct HostSpace {};
+struct LayoutRight {};
+struct Atomic {};
+template <class T> struct MemoryTraits {};
+
+struct ViewAllocateWithoutInitializing {
+    std::string label;
+    explicit ViewAllocateWithoutInitializing(const std::string &l) : label(l) {}
+};
+
+namespace shim_detail {
+template <class T> struct rank_of { static constexpr int value = 0; using value_type = T; };
+template <class T> struct rank_of<T *> {
+    static constexpr int value = 1 + rank_of<T>::value;
+    using value_type = typename rank_of<T>::value_type;
+};
+struct Storage {
+    void *ptr = nullptr;
+    ~Storage() { std::free(ptr); }
+};
+} // namespace shim_detail
+
+template <class DataType, class... Props> class View {
+  public:
+    static constexpr int Rank = shim_detail::rank_of<DataType>::value;
+    using value_type = typename shim_detail::rank_of<DataType>::value_type;
+    using non_const_value_type = typename std::remove_const<value_type>::type;
+
+    View() = default;
+    View(const ViewAllocateWithoutInitializing &a, size_t n0 = 0, size_t n1 = 0, size_t n2 = 0) {
+        allocate(a.label, n0, n1, n2);
+    }
+    View(const std::string &label, size_t n0 = 0, size_t n1 = 0, size_t n2 = 0) { allocate(label, n0, n1, n2); }
+    View(const char *label, size_t n0 = 0, size_t n1 = 0, size_t n2 = 0) {
+        allocate(std::string(label), n0, n1, n2);
+    }
+    template <class... P2>
+    View(const View<DataType, P2...> &o) : store_(o.store_), data_(o.data_), label_(o.label_) {
+        ext_[0] = o.ext_[0];
+        ext_[1] = o.ext_[1];
+        ext_[2] = o.ext_[2];
+    }
+
+    value_type *data() const { return data_; }
+    size_t extent(int r) const { return ext_[r]; }
+    size_t size() const {
+        size_t s = 1;
+        for (int r = 0; r < Rank; r++)
+            s *= ext_[r];
+        return Rank == 0 ? 1 : s;
+    }
+    size_t span() const { return size(); }
+    const std::string &label() const { return label_; }
+
+    value_type &operator()() const { return data_[0]; }
+    template <class I0> value_type &operator()(I0 i) const { return data_[(size_t)i]; }
+    template <class I0, class I1> value_type &operator()(I0 i, I1 j) const {
+        return data_[(size_t)i * ext_[1] + (size_t)j];
+    }
+    template <class I0, class I1, class I2> value_type &operator()(I0 i, I1 j, I2 k) const {
+        return data_[((size_t)i * ext_[1] + (size_t)j) * ext_[2] + (size_t)k];
+    }
+    template <class I0> value_type &operator[](I0 i) const { return data_[(size_t)i]; }
+
+    void allocate(const std::string &label, size_t n0, size_t n1, size_t n2) {
+        label_ = label;
+        ext_[0] = n0;
+        ext_[1] = Rank >= 2 ? n1 : 1;
+        ext_[2] = Rank >= 3 ? n2 : 1;
+        if (Rank < 2)
+            ext_[1] = 0;
+        if (Rank < 3)
+            ext_[2] = 0;
+        size_t n = size();
+        store_ = std::make_shared<shim_detail::Storage>();
+        store_->ptr = std::calloc(n == 0 ? 1 : n, sizeof(value_type));
+        if (!store_->ptr)
+            throw std::runtime_error("shim View allocation failed: " + label);
+        data_ = static_cast<value_type *>(store_->ptr);
+    }
+
+    std::shared_ptr<shim_detail::Storage> store_;
+    value_type *data_ = nullptr;
+    size_t ext_[3] = {0, 0, 0};
+    std::string label_;
+};
+
+template <class DataType, class... P> void resize(View<DataType, P...> &v, size_t n0, size_t n1 = 0, size_t n2 = 0) {
+    View<DataType, P...> nv(v.label(), n0, n1, n2);
+    constexpr int R = View<DataType, P...>::Rank;
+    if (v.data() != nullptr) {
+        if (R == 1) {
+            size_t m = std::min(v.extent(0), n0);
+            std::memcpy(nv.data(), v.data(), m * sizeof(typename View<DataType, P...>::value_type));
+        }
+        else if (R == 2) {
+            for (size_t i = 0; i < std::min(v.extent(0), n0); i++)
+                for (size_t j = 0; j < std::min(v.extent(1), n1); j++)
+                    nv(i, j) = v(i, j);
+        }
+        else {
+            for (size_t i = 0; i < std::min(v.extent(0), n0); i++)
+                for (size_t j = 0; j < std::min(v.extent(1), n1); j++)
+                    for (size_t k = 0; k < std::min(v.extent(2), n2); k++)
+                        nv(i, j, k) = v(i, j, k);
+        }
+    }
+    v = nv;
+}
+
+template <class D1, class... P1, class D2, class... P2>
+void deep_copy(const View<D1, P1...> &dst, const View<D2, P2...> &src) {
+    if ((void *)dst.data() == (void *)src.data())
+        return;
+    size_t n = std::min(dst.size(), src.size());
+    std::memmove(dst.data(), src.data(), n * sizeof(typename View<D1, P1...>::value_type));
+}
+template <class D1, class... P1, class S,
+          class = typename std::enable_if<std::is_arithmetic<S>::value>::type>
+void deep_copy(const View<D1, P1...> &dst, const S &val) {
+    using T = typename View<D1, P1...>::value_type;
+    T v = (T)val;
+    for (size_t i = 0; i < dst.size(); i++)
+        dst.data()[i] = v;
+}
+
+template <class Space, class D, class... P> View<D, P...> create_mirror_view_and_copy(const Space &, const View<D, P...> &v) {
+    return v;
+}
+
+struct Serial {
+    using memory_space = HostSpace;
+    using execution_space = Serial;
+    using array_layout = LayoutRight;
+    static void print_configuration(std::ostream &os) {
+#ifdef EXACA_SHIM_OPENMP
+        os << "Kokkos subset shim: OpenMP dispatch, " << omp_get_max_threads() << " threads" << std::endl;
+#else
+        os << "Kokkos subset shim: Serial dispatch" << std::endl;
+#endif
+    }
+};
+using DefaultExecutionSpace = Serial;
+
+inline void initialize(int &, char **) {}
+inline void finalize() {}
+inline void fence() {}
+
+template <class T> T atomic_fetch_add(T *p, T v) { return __atomic_fetch_add(p, v, __ATOMIC_SEQ_CST); }
+template <class T> T atomic_compare_exchange(T *p, T expected, T desired) {
+    __atomic_compare_exchange_n(p, &expected, desired, false, __ATOMIC_SEQ_CST, __ATOMIC_SEQ_CST);
+    return expected;
+}
+
+template <class T> struct reduction_identity {
+    static T sum() { return T(0); }
+    static T min() { return std::numeric_limits<T>::max(); }
+    static T max() { return std::numeric_limits<T>::lowest(); }
+};
+
+template <class T> struct Sum {
+    T &ref;
+    explicit Sum(T &r) : ref(r) {}
+    static T init() { return reduction_identity<T>::sum(); }
+    static void join(T &a, const T &b) { a += b; }
+};
+template <class T> struct Min {
+    T &ref;
+    explicit Min(T &r) : ref(r) {}
+    static T init() { return reduction_identity<T>::min(); }
+    static void join(T &a, const T &b) {
+        if (b < a)
+            a = b;
+    }
+};
+template <class T> struct Max {
+    T &ref;
+    explicit Max(T &r) : ref(r) {}
+    static T init() { return reduction_identity<T>::max(); }
+    static void join(T &a, const T &b) {
+        if (a < b)
+            a = b;
+    }
+};
+
+namespace Iterate {
+struct Right {};
+} // namespace Iterate
+template <int N, class O1 = Iterate::Right, class O2 = Iterate::Right> struct Rank {};
+template <class R> struct MDRangePolicy {
+    long lo[3], hi[3];
+    MDRangePolicy(std::initializer_list<long> l, std::initializer_list<long> h) {
+        int i = 0;
+        for (long v : l)
+            lo[i++] = v;
+        i = 0;
+        for (long v : h)
+            hi[i++] = v;
+    }
+};
+
+// parallel_for over [0, n)
+template <class F> void parallel_for(const std::string &, long n, const F &f) {
+#ifdef EXACA_SHIM_OPENMP
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < n; i++)
+        f(i);
+#else
+    for (long i = 0; i < n; i++)
+        f(i);
+#endif
+}
+template <class F> void parallel_for(long n, const F &f) { parallel_for(std::string(), n, f); }
+
+template <class R, class F> void parallel_for(const std::string &, const MDRangePolicy<R> &p, const F &f) {
+#ifdef EXACA_SHIM_OPENMP
+#pragma omp parallel for collapse(2) schedule(static)
+#endif
+    for (long k = p.lo[0]; k < p.hi[0]; k++)
+        for (long i = p.lo[1]; i < p.hi[1]; i++)
+            for (long j = p.lo[2]; j < p.hi[2]; j++)
+                f((int)k, (int)i, (int)j);
+}
+
+namespace shim_detail {
+template <class T, class Reducer, class F> void reduce_impl(long n, const F &f, T &out) {
+#ifdef EXACA_SHIM_OPENMP
+    T total = Reducer::init();
+#pragma omp parallel
+    {
+        T local = Reducer::init();
+#pragma omp for schedule(static)
+        for (long i = 0; i < n; i++)
+            f(i, local);
+#pragma omp critical
+        Reducer::join(total, local);
+    }
+    out = total;
+#else
+    T local = Reducer::init();
+    for (long i = 0; i < n; i++)
+        f(i, local);
+    out = local;
+#endif
+}
+} // namespace shim_detail
+
+// parallel_reduce with a plain scalar result (sum)
+template <class F, class T, class = typename std::enable_if<std::is_arithmetic<T>::value>::type>
+void parallel_reduce(const std::string &, long n, const F &f, T &result) {
+    shim_detail::reduce_impl<T, Sum<T>>(n, f, result);
+}
+template <class F, class T> void parallel_reduce(const std::string &, long n, const F &f, Sum<T> r) {
+    shim_detail::reduce_impl<T, Sum<T>>(n, f, r.ref);
+}
+template <class F, class T> void parallel_reduce(const std::string &, long n, const F &f, Min<T> r) {
+    shim_detail::reduce_impl<T, Min<T>>(n, f, r.ref);
+}
+template <class F, class T> void parallel_reduce(const std::string &, long n, const F &f, Max<T> r) {
+    shim_detail::reduce_impl<T, Max<T>>(n, f, r.ref);
+}
+template <class F, class T> void parallel_reduce(long n, const F &f, Sum<T> r) {
+    shim_detail::reduce_impl<T, Sum<T>>(n, f, r.ref);
+}
+
+} // namespace Kokkos
+
+#endif
