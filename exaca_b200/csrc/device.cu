@@ -1,0 +1,1093 @@
+// B200 kernels and pool runtime for ExaCA's per-cycle cellular-automaton update.
+//
+// One CA cycle (src/runCA.cpp:290-341; src/CAupdate.cpp:67-728) is three kernels over a pool of
+// domains:
+//   k_step_begin   per domain: device-side termination check, cycle/epoch advance, nucleation of
+//                  the sites whose time has come (nuclei are pre-sorted by time, one cursor each).
+//   k_grow_claim   per active cell of the shared compacted list: diagonal-length growth from the
+//                  host-built increment table, then every liquid neighbour it reaches is claimed
+//                  with a 64-bit atomicMin of (epoch, capturer index).
+//   k_capture      per active cell again: each claim it won becomes a capture (new decentred
+//                  octahedron and 26 critical diagonal lengths); it solidifies when no neighbour it
+//                  would have seen as liquid in the reference's serial order remains.
+// The claim rule reproduces the Kokkos-Serial loop order exactly: serial visits active cells in
+// ascending index and captures flip Liquid to Active in place, so the capturer of a cell is the
+// lowest-index claimant and an active cell sees a neighbour as liquid iff it was liquid at the start
+// of the cycle and no lower-index cell claimed it.
+//
+// Arithmetic follows the reference's types and operation order; this file is compiled with
+// -fmad=false so no multiply-add is contracted, and sqrt/division are IEEE round-to-nearest.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <climits>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <sstream>
+#include <stdexcept>
+
+#include "pool.hpp"
+
+namespace exaca {
+
+#define CUDA_OK(x)                                                                                                     \
+    do {                                                                                                               \
+        cudaError_t e__ = (x);                                                                                         \
+        if (e__ != cudaSuccess)                                                                                        \
+            throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(e__) + " at " #x);              \
+    } while (0)
+
+__constant__ int c_nx[26];
+__constant__ int c_ny[26];
+__constant__ int c_nz[26];
+__constant__ int c_itlist[9][26];
+__constant__ int c_itlen[9];
+
+constexpr unsigned int kMaskCarry = 1u << 30; // not eligible this cycle: keep in the list
+constexpr unsigned int kMaskDrop = 1u << 31;  // domain finished: leave the list
+constexpr int kErrGrowthTable = 1;
+constexpr int kErrListOverflow = 2;
+constexpr int kErrBounds = 4;
+constexpr int kErrJumps = 8;
+
+__device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; } // std::min
+__device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; } // std::max
+
+// Number of executed cycles in [1, x]: cycles skipped by the type-S/R jump
+// (src/CAupdate.cpp:812-817) are not executed and add no undercooling.
+__device__ __forceinline__ long long executed_upto(const DomainDesc &D, long long x) {
+    if (x <= 0)
+        return 0;
+    long long e = x;
+    for (int j = 0; j < D.n_jumps; j++) {
+        long long lo = D.jump_lo[j], hi = D.jump_hi[j];
+        if (x > lo)
+            e -= (x < hi ? x : hi) - lo;
+    }
+    return e;
+}
+
+// Warp-aggregated append of `n` entries per lane; returns this lane's base (or ULLONG_MAX on overflow).
+__device__ __forceinline__ unsigned long long warp_reserve(PoolState *P, int slot, unsigned int n) {
+    unsigned int lane = threadIdx.x & 31;
+    unsigned int incl = n;
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o)
+            incl += v;
+    }
+    unsigned int total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long base = 0;
+    if (lane == 31 && total)
+        base = atomicAdd(&P->cnt[slot], (unsigned long long)total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    if (base + total > P->capacity) {
+        if (lane == 0 && total)
+            atomicOr(&P->error, kErrListOverflow);
+        return ULLONG_MAX;
+    }
+    return base + (incl - n);
+}
+
+// Warp-aggregated per-domain counter update (lanes grouped by domain id).
+__device__ __forceinline__ void warp_add_domain(DomainDesc *desc, unsigned int dom, long long v,
+                                                unsigned long long DomainDesc::*field) {
+    unsigned int peers = __match_any_sync(0xffffffffu, dom);
+    int leader = __ffs(peers) - 1;
+    long long sum = 0;
+    for (unsigned int m = peers; m; m &= m - 1) {
+        int src = __ffs(m) - 1;
+        sum += __shfl_sync(peers, v, src);
+    }
+    if ((int)(threadIdx.x & 31) == leader && sum)
+        atomicAdd(&(desc[dom].*field), (unsigned long long)sum);
+}
+
+__device__ __forceinline__ void warp_add_liquid(DomainDesc *desc, unsigned int dom, long long v) {
+    unsigned int peers = __match_any_sync(0xffffffffu, dom);
+    int leader = __ffs(peers) - 1;
+    long long sum = 0;
+    for (unsigned int m = peers; m; m &= m - 1) {
+        int src = __ffs(m) - 1;
+        sum += __shfl_sync(peers, v, src);
+    }
+    if ((int)(threadIdx.x & 31) == leader && sum)
+        atomicAdd((unsigned long long *)&desc[dom].liquid, (unsigned long long)(-sum));
+}
+
+// Fresh octahedron of a newly active cell at its own centre (src/CAupdate.cpp:100-194,
+// src/CAinitialize.cpp:1942-2042): DL = 0.01, centre = cell centre, CDL from the orientation table.
+__device__ void make_fresh_octahedron(const DomainDesc &D, long long c) {
+    int plane = D.mx * D.my;
+    int rz = (int)(c / plane);
+    int rem = (int)(c - (long long)rz * plane);
+    int rx = rem / D.my, ry = rem - (rem / D.my) * D.my;
+    int h = D.gid[c];
+    int ori = (abs(h) - 1) % 10000;
+    if (ori < 0)
+        ori += 10000;
+    D.dl[c] = 0.01f;
+    D.doc[3 * c + 0] = (float)((double)(rx + D.xoff) + 0.5);
+    D.doc[3 * c + 1] = (float)((double)(ry + D.yoff) + 0.5);
+    D.doc[3 * c + 2] = (float)((double)rz + 0.5);
+    const float *t = D.cdl_table + 26 * ori;
+    float *o = D.cdl + 26 * c;
+#pragma unroll
+    for (int n = 0; n < 26; n++)
+        o[n] = t[n];
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_step_begin: one block; warp w serves domains w, w + nwarps, ...
+__global__ void k_step_begin(PoolState *P) {
+    __shared__ int s_cur;
+    if (threadIdx.x == 0) {
+        // the list built by the previous cycle becomes current; the consumed one is reset
+        int cur = P->cur ^ 1;
+        P->cur = cur;
+        P->cnt[cur ^ 1] = 0;
+        s_cur = cur;
+    }
+    __syncthreads();
+    int cur = s_cur;
+    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    for (int d = warp; d < P->n_domains; d += nwarps) {
+        DomainDesc &D = P->desc[d];
+        if (D.ctype == nullptr || D.done)
+            continue;
+        if (D.check_mode && D.cycle > 0 && D.cycle % 1000 == 0 && D.liquid == 0) {
+            // src/CAupdate.cpp:782-783: no superheated or undercooled liquid left
+            if (lane == 0)
+                D.done = 1;
+            continue;
+        }
+        int cycle = D.cycle + 1;
+        __syncwarp();
+        if (lane == 0) {
+            D.cycle = cycle;
+            D.epoch = D.epoch + 1;
+        }
+        // src/CAupdate.cpp:76-198: sites with cycle >= NucleationTimes that are still liquid
+        int cursor = D.nuc_cursor;
+        int fired_total = 0;
+        while (cursor < D.n_nuclei) {
+            int idx = cursor + lane;
+            int t = idx < D.n_nuclei ? D.nuc_time[idx] : INT_MAX;
+            unsigned int due = __ballot_sync(0xffffffffu, t <= cycle);
+            // nuclei are sorted by time, so the due ones form a prefix
+            int n_due = __popc(due);
+            bool fire = false;
+            long long loc = 0;
+            if (t <= cycle) {
+                loc = D.nuc_loc[idx];
+                if (loc < 0 || loc >= D.active_size) {
+                    atomicOr(&D.error, kErrBounds);
+                    loc = 0;
+                }
+                else {
+                    fire = D.ctype[loc] == kLiquid && D.layer[loc] <= 0;
+                }
+                if (fire)
+                    make_fresh_octahedron(D, loc);
+            }
+            unsigned int fired = __ballot_sync(0xffffffffu, fire);
+            if (fire) {
+                int rank = __popc(fired & ((1u << lane) - 1));
+                unsigned long long base = 0;
+                if (rank == 0)
+                    base = atomicAdd(&P->cnt[cur], (unsigned long long)__popc(fired));
+                base = __shfl_sync(fired, base, __ffs(fired) - 1);
+                if (base + __popc(fired) > P->capacity) {
+                    atomicOr(&P->error, kErrListOverflow);
+                }
+                else {
+                    P->list[cur][base + rank] = ((unsigned long long)d << 32) | (unsigned long long)loc;
+                }
+                __threadfence();
+                D.ctype[loc] = kActive;
+            }
+            fired_total += __popc(fired);
+            cursor += n_due;
+            if (n_due < 32)
+                break;
+        }
+        if (lane == 0) {
+            D.nuc_cursor = cursor;
+            D.nn += fired_total;
+            D.liquid -= fired_total;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// k_grow_claim: src/CAupdate.cpp:217-352 for every listed active cell
+__global__ void __launch_bounds__(256) k_grow_claim(PoolState *P) {
+    const int cur = P->cur;
+    const unsigned long long n = P->cnt[cur];
+    const unsigned long long *list = P->list[cur];
+    unsigned int *mask = P->mask;
+    DomainDesc *desc = P->desc;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i0 = (unsigned long long)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        unsigned long long i = i0 + threadIdx.x;
+        bool valid = i < n;
+        unsigned int dom = 0;
+        long long grown = 0;
+        if (valid) {
+            unsigned long long e = list[i];
+            dom = (unsigned int)(e >> 32);
+            long long c = (long long)(e & 0xffffffffull);
+            DomainDesc &D = desc[dom];
+            unsigned int m;
+            if (D.done) {
+                m = kMaskDrop;
+            }
+            else {
+                int cycle = D.cycle;
+                int cts = D.cts[c];
+                if (!(cycle > cts) || D.layer[c] > 0) {
+                    m = kMaskCarry;
+                }
+                else {
+                    grown = 1;
+                    long long nu = 0;
+                    if (D.du[c] != 0.0f)
+                        nu = executed_upto(D, cycle) - executed_upto(D, cts);
+                    double inc = 0.0;
+                    if (nu >= 0 && nu < D.growth_len)
+                        inc = __ldg(D.growth + nu);
+                    else
+                        atomicOr(&D.error, kErrGrowthTable);
+                    float dl = (float)((double)D.dl[c] + inc);
+                    D.dl[c] = dl;
+                    int plane = D.mx * D.my;
+                    int rz = (int)(c / plane);
+                    int rem = (int)(c - (long long)rz * plane);
+                    int rx = rem / D.my;
+                    int ry = rem - rx * D.my;
+                    int b = (ry == 0) ? (rx == 0 ? 5 : (rx == D.mx - 1 ? 6 : 1))
+                                      : (ry == D.my - 1 ? (rx == 0 ? 7 : (rx == D.mx - 1 ? 8 : 2))
+                                                        : (rx == 0 ? 3 : (rx == D.mx - 1 ? 4 : 0)));
+                    unsigned long long key =
+                        ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
+                    const float *cdl = D.cdl + 26 * c;
+                    unsigned int liq = 0;
+                    int len = c_itlen[b];
+                    for (int ll = 0; ll < len; ll++) {
+                        int l = c_itlist[b][ll];
+                        int nzz = rz + c_nz[l];
+                        if (nzz >= D.nz_active || nzz < 0)
+                            continue;
+                        long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
+                        if (D.ctype[t] == kLiquid) {
+                            liq |= 1u << l;
+                            if (dl >= cdl[l])
+                                atomicMin(&D.claim[t], key);
+                        }
+                    }
+                    m = liq;
+                }
+            }
+            mask[i] = m;
+        }
+        warp_add_domain(desc, valid ? dom : 0xffffffffu, grown, &DomainDesc::n_grown);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Capture of liquid cell t by active cell c through neighbour direction l
+// (src/CAupdate.cpp:353-563, 713-717).
+__device__ void capture_cell(const DomainDesc &D, long long c, long long t, int l) {
+    int plane = D.mx * D.my;
+    int rz = (int)(c / plane);
+    int rem = (int)(c - (long long)rz * plane);
+    int rx = rem / D.my;
+    int ry = rem - rx * D.my;
+    int GlobalX = rx + D.xoff, GlobalY = ry + D.yoff, GlobalZ = rz;
+    int h = D.gid[c];
+    int ori = (abs(h) - 1) % 10000;
+    if (ori < 0)
+        ori += 10000;
+    const float *g = D.guv + 9 * ori;
+    const float g0 = g[0], g1 = g[1], g2 = g[2], g3 = g[3], g4 = g[4], g5 = g[5], g6 = g[6], g7 = g[7], g8 = g[8];
+    D.gid[t] = h;
+    double cxold = D.doc[3 * c + 0];
+    double cyold = D.doc[3 * c + 1];
+    double czold = D.doc[3 * c + 2];
+    double xp = GlobalX + c_nx[l] + 0.5;
+    double yp = GlobalY + c_ny[l] + 0.5;
+    double zp = GlobalZ + c_nz[l] + 0.5;
+    double x0 = xp - cxold;
+    double y0 = yp - cyold;
+    double z0 = zp - czold;
+    double mag0 = sqrtf((float)(x0 * x0 + y0 * y0 + z0 * z0));
+    double Angle1 = (g0 * x0 + g1 * y0 + g2 * z0) / mag0;
+    double Angle2 = (g3 * x0 + g4 * y0 + g5 * z0) / mag0;
+    double Angle3 = (g6 * x0 + g7 * y0 + g8 * z0) / mag0;
+    float s1 = (float)(2 * (Angle1 < 0) - 1);
+    float s2 = (float)(2 * (Angle2 < 0) - 1);
+    float s3 = (float)(2 * (Angle3 < 0) - 1);
+    double Diag1X = g0 * s1, Diag1Y = g1 * s1, Diag1Z = g2 * s1;
+    double Diag2X = g3 * s2, Diag2Y = g4 * s2, Diag2Z = g5 * s2;
+    double Diag3X = g6 * s3, Diag3Y = g7 * s3, Diag3Z = g8 * s3;
+    double U1x = Diag2X - Diag1X, U1y = Diag2Y - Diag1Y, U1z = Diag2Z - Diag1Z;
+    double U2x = Diag3X - Diag1X, U2y = Diag3Y - Diag1Y, U2z = Diag3Z - Diag1Z;
+    double UUx = U1y * U2z - U1z * U2y;
+    double UUy = U1z * U2x - U1x * U2z;
+    double UUz = U1x * U2y - U1y * U2x;
+    double NDem = sqrtf((float)(UUx * UUx + UUy * UUy + UUz * UUz));
+    double n0 = UUx / NDem, n1 = UUy / NDem, n2 = UUz / NDem;
+    double ParaT = (n0 * x0 + n1 * y0 + n2 * z0) / (n0 * Diag1X + n1 * Diag1Y + n2 * Diag1Z);
+    double TX[3], TY[3], TZ[3];
+    TX[0] = cxold + ParaT * Diag1X;
+    TY[0] = cyold + ParaT * Diag1Y;
+    TZ[0] = czold + ParaT * Diag1Z;
+    TX[1] = cxold + ParaT * Diag2X;
+    TY[1] = cyold + ParaT * Diag2Y;
+    TZ[1] = czold + ParaT * Diag2Z;
+    TX[2] = cxold + ParaT * Diag3X;
+    TY[2] = cyold + ParaT * Diag3Y;
+    TZ[2] = czold + ParaT * Diag3Z;
+    double Dist[3];
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+        Dist[q] = sqrtf((float)(((TX[q] - xp) * (TX[q] - xp)) + ((TY[q] - yp) * (TY[q] - yp)) +
+                                ((TZ[q] - zp) * (TZ[q] - zp))));
+    int x = (Dist[0] < Dist[1]);
+    int y = (Dist[1] < Dist[2]);
+    int z = (Dist[2] < Dist[0]);
+    int idx = 2 * (z - y) * z + (y - x) * y;
+    double mindist = Dist[idx];
+    double xc = TX[idx], yc = TY[idx], zc = TZ[idx];
+    int i1 = (idx + 1) % 3, i2 = (idx + 2) % 3;
+    double x1 = TX[i1], y1 = TY[i1], z1 = TZ[i1];
+    double x2 = TX[i2], y2 = TY[i2], z2 = TZ[i2];
+    double D1 = sqrtf((float)(((xp - x2) * (xp - x2)) + ((yp - y2) * (yp - y2)) + ((zp - z2) * (zp - z2))));
+    double D2 = sqrtf((float)(((xc - x2) * (xc - x2)) + ((yc - y2) * (yc - y2)) + ((zc - z2) * (zc - z2))));
+    double D3 = sqrtf((float)(((xp - x1) * (xp - x1)) + ((yp - y1) * (yp - y1)) + ((zp - z1) * (zp - z1))));
+    double D4 = sqrtf((float)(((xc - x1) * (xc - x1)) + ((yc - y1) * (yc - y1)) + ((zc - z1) * (zc - z1))));
+    double I1 = 0, I2 = D2, J1 = 0, J2 = D4;
+    if (mindist != 0) {
+        I1 = D1 * ((xp - x2) * (xc - x2) + (yp - y2) * (yc - y2) + (zp - z2) * (zc - z2)) / (D1 * D2);
+        I2 = D2 - I1;
+        J1 = D3 * ((xp - x1) * (xc - x1) + (yp - y1) * (yc - y1) + (zp - z1) * (zc - z1)) / (D3 * D4);
+        J2 = D4 - J1;
+    }
+    const double sqrt3 = sqrt(3.0);
+    double L12 = 0.5 * (dmin(I1, sqrt3) + dmin(I2, sqrt3));
+    double L13 = 0.5 * (dmin(J1, sqrt3) + dmin(J2, sqrt3));
+    double NewODiagL = sqrt(2.0) * dmax(L12, L13);
+    D.dl[t] = (float)NewODiagL;
+    double cd0 = xc - cxold, cd1 = yc - cyold, cd2 = zc - czold;
+    double nd = sqrt(cd0 * cd0 + cd1 * cd1 + cd2 * cd2);
+    double uv0 = cd0 / nd, uv1 = cd1 / nd, uv2 = cd2 / nd;
+    double cx = xc - NewODiagL * uv0;
+    double cy = yc - NewODiagL * uv1;
+    double cz = zc - NewODiagL * uv2;
+    D.doc[3 * t + 0] = (float)cx;
+    D.doc[3 * t + 1] = (float)cy;
+    D.doc[3 * t + 2] = (float)cz;
+    // face normals: float sums of the unit-vector components (src/CAupdate.cpp:526-551)
+    double Fx[4], Fy[4], Fz[4];
+    Fx[0] = g0 + g3 + g6;
+    Fx[1] = g0 - g3 + g6;
+    Fx[2] = g0 + g3 - g6;
+    Fx[3] = g0 - g3 - g6;
+    Fy[0] = g1 + g4 + g7;
+    Fy[1] = g1 - g4 + g7;
+    Fy[2] = g1 + g4 - g7;
+    Fy[3] = g1 - g4 - g7;
+    Fz[0] = g2 + g5 + g8;
+    Fz[1] = g2 - g5 + g8;
+    Fz[2] = g2 + g5 - g8;
+    Fz[3] = g2 - g5 - g8;
+    float *out = D.cdl + 26 * t;
+#pragma unroll 2
+    for (int n = 0; n < 26; n++) {
+        double a0 = xp + c_nx[n] - cx;
+        double b0 = yp + c_ny[n] - cy;
+        double d0 = zp + c_nz[n] - cz;
+        double q0 = a0 * Fx[0] + b0 * Fy[0] + d0 * Fz[0];
+        double q1 = a0 * Fx[1] + b0 * Fy[1] + d0 * Fz[1];
+        double q2 = a0 * Fx[2] + b0 * Fy[2] + d0 * Fz[2];
+        double q3 = a0 * Fx[3] + b0 * Fy[3] + d0 * Fz[3];
+        double m = dmax(dmax(fabs(q0), fabs(q1)), dmax(fabs(q2), fabs(q3)));
+        out[n] = (float)m;
+    }
+}
+
+// k_capture: captures won, solidification (src/CAupdate.cpp:336-352, 722-725), next list.
+__global__ void __launch_bounds__(256) k_capture(PoolState *P) {
+    const int cur = P->cur;
+    const int nxt = cur ^ 1;
+    const unsigned long long n = P->cnt[cur];
+    const unsigned long long *list = P->list[cur];
+    unsigned long long *out = P->list[nxt];
+    const unsigned int *mask = P->mask;
+    DomainDesc *desc = P->desc;
+    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+    for (unsigned long long i0 = (unsigned long long)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
+        unsigned long long i = i0 + threadIdx.x;
+        bool valid = i < n;
+        unsigned int dom = 0xffffffffu;
+        unsigned long long e = 0;
+        unsigned int m = kMaskDrop;
+        if (valid) {
+            e = list[i];
+            dom = (unsigned int)(e >> 32);
+            m = mask[i];
+        }
+        // captured targets of this lane, as neighbour directions
+        unsigned int won = 0;
+        bool keep = false;
+        long long c = (long long)(e & 0xffffffffull);
+        if (valid && !(m & kMaskDrop)) {
+            if (m & kMaskCarry) {
+                keep = true;
+            }
+            else {
+                const DomainDesc &D = desc[dom];
+                int plane = D.mx * D.my;
+                unsigned int want = 0xffffffffu - D.epoch;
+                bool lcount = false;
+                for (unsigned int bits = m; bits; bits &= bits - 1) {
+                    int l = __ffs(bits) - 1;
+                    long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
+                    unsigned long long k = D.claim[t];
+                    if ((unsigned int)(k >> 32) == want) {
+                        long long w = (long long)(k & 0xffffffffull);
+                        if (w >= c)
+                            lcount = true;
+                        if (w == c)
+                            won |= 1u << l;
+                    }
+                    else {
+                        lcount = true;
+                    }
+                }
+                for (unsigned int bits = won; bits; bits &= bits - 1) {
+                    int l = __ffs(bits) - 1;
+                    long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
+                    capture_cell(D, c, t, l);
+                }
+                if (!lcount)
+                    D.ctype[c] = kSolid;
+                keep = lcount;
+            }
+        }
+        unsigned int n_out = (keep ? 1u : 0u) + (unsigned int)__popc(won);
+        unsigned long long base = warp_reserve(P, nxt, n_out);
+        if (base != ULLONG_MAX && n_out) {
+            unsigned long long hi = (unsigned long long)dom << 32;
+            unsigned long long pos = base;
+            if (keep)
+                out[pos++] = e;
+            if (won) {
+                const DomainDesc &D = desc[dom];
+                int plane = D.mx * D.my;
+                for (unsigned int bits = won; bits; bits &= bits - 1) {
+                    int l = __ffs(bits) - 1;
+                    long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
+                    out[pos++] = hi | (unsigned long long)t;
+                }
+            }
+        }
+        // set the captured cells active only after their octahedron data is written
+        if (won) {
+            const DomainDesc &D = desc[dom];
+            int plane = D.mx * D.my;
+            __threadfence();
+            for (unsigned int bits = won; bits; bits &= bits - 1) {
+                int l = __ffs(bits) - 1;
+                long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
+                D.ctype[t] = kActive;
+            }
+        }
+        long long ncap = __popc(won);
+        warp_add_domain(desc, dom, ncap, &DomainDesc::n_captured);
+        warp_add_liquid(desc, dom, ncap);
+        warp_add_domain(desc, dom, valid ? 1 : 0, &DomainDesc::n_listed);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Census of src/CAupdate.cpp:738-808 for one domain (layer 0 is the only layer).
+__global__ void k_census(const DomainDesc *Dp, Census *out) {
+    const DomainDesc &D = *Dp;
+    unsigned long long a[5] = {0, 0, 0, 0, 0};
+    unsigned long long mn = ULLONG_MAX;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    int cycle = D.cycle;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < D.domain_size; c += stride) {
+        int t = D.ctype[c];
+        int ly = D.layer[c];
+        int cts = D.cts[c];
+        if (ly == 0) {
+            if (t == kLiquid) {
+                if (cts > cycle)
+                    a[0]++;
+                else
+                    a[1]++;
+                if (c < D.active_size && (unsigned long long)cts < mn)
+                    mn = (unsigned long long)(long long)cts;
+            }
+            else if (t == kActive)
+                a[2]++;
+            else if (t == kSolid)
+                a[3]++;
+        }
+        else if (t == kLiquid) {
+            a[4]++;
+        }
+    }
+    for (int q = 0; q < 5; q++) {
+        unsigned long long v = a[q];
+        for (int o = 16; o; o >>= 1)
+            v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v)
+            atomicAdd((unsigned long long *)out + q, v);
+    }
+    for (int o = 16; o; o >>= 1) {
+        unsigned long long v = __shfl_down_sync(0xffffffffu, mn, o);
+        mn = v < mn ? v : mn;
+    }
+    if ((threadIdx.x & 31) == 0)
+        atomicMin(&out->next_cts, mn);
+}
+
+// Voronoi baseplate (src/CAinitialize.cpp:1646-1677): nearest seed by float distance, the first
+// seed in draw order wins ties.
+__global__ void k_voronoi(DomainDesc *Dp, const int32_t *seeds, int nseeds, float init_min) {
+    extern __shared__ int s_seed[];
+    const DomainDesc &D = *Dp;
+    long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    bool mine = c < D.domain_size && D.gid[c] == kVoronoiPending;
+    int gx = 0, gy = 0, k = 0;
+    if (mine) {
+        int plane = D.mx * D.my;
+        k = (int)(c / plane);
+        int rem = (int)(c - (long long)k * plane);
+        gx = rem / D.my + D.xoff;
+        gy = rem % D.my + D.yoff;
+    }
+    float best = init_min;
+    int best_i = -1;
+    for (int base = 0; base < nseeds; base += 1024) {
+        int cnt = min(1024, nseeds - base);
+        __syncthreads();
+        for (int q = threadIdx.x; q < 3 * cnt; q += blockDim.x)
+            s_seed[q] = seeds[3 * base + q];
+        __syncthreads();
+        if (mine) {
+            for (int q = 0; q < cnt; q++) {
+                float dx = (float)(abs(s_seed[3 * q] - gx));
+                float dy = (float)(abs(s_seed[3 * q + 1] - gy));
+                float dz = (float)(abs(s_seed[3 * q + 2] - k));
+                float dist = sqrtf(dx * dx + dy * dy + dz * dz);
+                if (dist < best) {
+                    best_i = base + q;
+                    best = dist;
+                }
+            }
+        }
+    }
+    if (mine)
+        D.gid[c] = best_i + 1;
+}
+
+// Initially active cells: fresh octahedra and the first active list (src/CAinitialize.cpp:1929-2044).
+__global__ void k_init_active(PoolState *P, int dom, int list_slot) {
+    DomainDesc &D = P->desc[dom];
+    long long plane = (long long)D.mx * D.my;
+    long long lo = plane, hi = plane * (D.nz - 1);
+    long long zmax = plane * ((long long)D.zbound_high + 1);
+    if (hi > zmax)
+        hi = zmax;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    for (long long c0 = lo + (long long)blockIdx.x * blockDim.x; c0 < hi; c0 += stride) {
+        long long c = c0 + threadIdx.x;
+        bool act = c < hi && D.ctype[c] == kActive;
+        if (act)
+            make_fresh_octahedron(D, c);
+        bool listed = act && c < D.active_size;
+        unsigned long long base = warp_reserve(P, list_slot, listed ? 1u : 0u);
+        if (listed && base != ULLONG_MAX)
+            P->list[list_slot][base] = ((unsigned long long)dom << 32) | (unsigned long long)c;
+    }
+}
+
+// Re-labels every entry of one domain in the list the next cycle consumes with the pool's
+// always-finished placeholder domain (used when a slot is retired, before the slot is reused).
+__global__ void k_drop_domain(PoolState *P, unsigned int dom, unsigned int placeholder) {
+    const int nxt = P->cur ^ 1;
+    unsigned long long n = P->cnt[nxt];
+    unsigned long long *list = P->list[nxt];
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x)
+        if ((unsigned int)(list[i] >> 32) == dom)
+            list[i] = (unsigned long long)placeholder << 32;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Pool runtime
+
+namespace {
+inline cudaStream_t S(void *s) { return (cudaStream_t)s; }
+template <class T> T *dalloc(size_t n, std::vector<void *> &allocs, size_t &bytes) {
+    void *p = nullptr;
+    size_t b = std::max<size_t>(n * sizeof(T), 16);
+    CUDA_OK(cudaMalloc(&p, b));
+    allocs.push_back(p);
+    bytes += b;
+    return (T *)p;
+}
+} // namespace
+
+size_t Pool::slot_bytes(const Problem &p) {
+    size_t N = (size_t)p.g.domain_size, A = (size_t)p.g.active_size;
+    return N * (1 + 4 + 4 + 1 + 4) + A * (4 + 12 + 104 + 8) + p.nuclei_loc.size() * 8 + 64 * 1024;
+}
+
+Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
+    : device_(device), budget_(budget_bytes) {
+    CUDA_OK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CUDA_OK(cudaGetDeviceProperties(&prop, device));
+    num_sms_ = prop.multiProcessorCount;
+    cudaStream_t s;
+    CUDA_OK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    stream_ = s;
+    int it[9][26], lens[9];
+    build_itlist(it, lens);
+    CUDA_OK(cudaMemcpyToSymbol(c_nx, kNeighborX, sizeof(kNeighborX)));
+    CUDA_OK(cudaMemcpyToSymbol(c_ny, kNeighborY, sizeof(kNeighborY)));
+    CUDA_OK(cudaMemcpyToSymbol(c_nz, kNeighborZ, sizeof(kNeighborZ)));
+    CUDA_OK(cudaMemcpyToSymbol(c_itlist, it, sizeof(it)));
+    CUDA_OK(cudaMemcpyToSymbol(c_itlen, lens, sizeof(lens)));
+    max_domains_ = 8192;
+    capacity_ = std::max<unsigned long long>(list_capacity, 1024);
+    CUDA_OK(cudaMalloc(&dstate_, sizeof(PoolState)));
+    CUDA_OK(cudaMalloc(&ddesc_, sizeof(DomainDesc) * (max_domains_ + 1)));
+    CUDA_OK(cudaMemset(ddesc_, 0, sizeof(DomainDesc) * (max_domains_ + 1)));
+    {
+        // descriptor max_domains_ is a placeholder that is always finished
+        DomainDesc ph;
+        std::memset(&ph, 0, sizeof(ph));
+        ph.done = 1;
+        CUDA_OK(cudaMemcpy(ddesc_ + max_domains_, &ph, sizeof(ph), cudaMemcpyHostToDevice));
+    }
+    PoolState ps;
+    std::memset(&ps, 0, sizeof(ps));
+    CUDA_OK(cudaMalloc(&ps.list[0], capacity_ * sizeof(unsigned long long)));
+    CUDA_OK(cudaMalloc(&ps.list[1], capacity_ * sizeof(unsigned long long)));
+    CUDA_OK(cudaMalloc(&ps.mask, capacity_ * sizeof(unsigned int)));
+    ps.capacity = capacity_;
+    ps.cur = 1; // k_step_begin flips to 0 on the first cycle
+    ps.n_domains = 0;
+    ps.desc = ddesc_;
+    CUDA_OK(cudaMemcpy(dstate_, &ps, sizeof(ps), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMalloc(&census_buf_, sizeof(Census)));
+}
+
+Pool::~Pool() {
+    cudaSetDevice(device_);
+    cudaStreamSynchronize(S(stream_));
+    if (graph_exec_)
+        cudaGraphExecDestroy((cudaGraphExec_t)graph_exec_);
+    for (auto &s : slots_) {
+        for (void *p : s.allocs)
+            cudaFree(p);
+        if (s.growth)
+            cudaFree(s.growth);
+    }
+    for (auto &kv : tables_) {
+        cudaFree(kv.second.guv);
+        cudaFree(kv.second.cdl_table);
+    }
+    if (dstate_) {
+        PoolState ps;
+        if (cudaMemcpy(&ps, dstate_, sizeof(ps), cudaMemcpyDeviceToHost) == cudaSuccess) {
+            cudaFree(ps.list[0]);
+            cudaFree(ps.list[1]);
+            cudaFree(ps.mask);
+        }
+        cudaFree(dstate_);
+    }
+    cudaFree(ddesc_);
+    cudaFree(census_buf_);
+    cudaStreamDestroy(S(stream_));
+}
+
+const DeviceTables &Pool::tables_for(const Problem &p) {
+    auto it = tables_.find(p.cfg.orientation_file);
+    if (it != tables_.end())
+        return it->second;
+    DeviceTables t;
+    CUDA_OK(cudaMalloc(&t.guv, p.guv.size() * sizeof(float)));
+    CUDA_OK(cudaMalloc(&t.cdl_table, p.cdl_table.size() * sizeof(float)));
+    CUDA_OK(cudaMemcpy(t.guv, p.guv.data(), p.guv.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaMemcpy(t.cdl_table, p.cdl_table.data(), p.cdl_table.size() * sizeof(float), cudaMemcpyHostToDevice));
+    return tables_[p.cfg.orientation_file] = t;
+}
+
+void Pool::push_desc(int slot) {
+    CUDA_OK(cudaMemcpyAsync(ddesc_ + slot, &host_desc_[slot], sizeof(DomainDesc), cudaMemcpyHostToDevice, S(stream_)));
+    CUDA_OK(cudaStreamSynchronize(S(stream_)));
+}
+
+void Pool::ensure_growth(int slot, long long needed) {
+    SlotHost &s = slots_[slot];
+    if (needed < s.growth_len)
+        return;
+    long long len = std::max<long long>(needed + 1, std::max<long long>(2LL * s.growth_len, 4096));
+    if (len > INT_MAX / 2)
+        throw std::runtime_error("growth table too long");
+    std::vector<double> g;
+    build_growth_table(*s.problem, (int)len, g);
+    double *d = nullptr;
+    CUDA_OK(cudaMalloc(&d, len * sizeof(double)));
+    CUDA_OK(cudaMemcpy(d, g.data(), len * sizeof(double), cudaMemcpyHostToDevice));
+    CUDA_OK(cudaStreamSynchronize(S(stream_)));
+    if (s.growth)
+        CUDA_OK(cudaFree(s.growth));
+    s.growth = d;
+    s.growth_len = (int)len;
+    // patch only the table fields of the device descriptor
+    DomainDesc &h = host_desc_[slot];
+    h.growth = d;
+    h.growth_len = (int)len;
+    CUDA_OK(cudaMemcpyAsync((char *)(ddesc_ + slot) + offsetof(DomainDesc, growth), &h.growth, sizeof(h.growth),
+                            cudaMemcpyHostToDevice, S(stream_)));
+    CUDA_OK(cudaMemcpyAsync((char *)(ddesc_ + slot) + offsetof(DomainDesc, growth_len), &h.growth_len,
+                            sizeof(h.growth_len), cudaMemcpyHostToDevice, S(stream_)));
+    CUDA_OK(cudaStreamSynchronize(S(stream_)));
+}
+
+int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
+    CUDA_OK(cudaSetDevice(device_));
+    const Problem &p = *pp;
+    if (p.g.zbound_low != 0)
+        throw std::runtime_error("active window must start at z = 0");
+    size_t need = slot_bytes(p);
+    if (bytes_in_use_ + need > budget_)
+        throw std::runtime_error("admission refused: HBM budget exceeded");
+    int slot = -1;
+    for (int s = 0; s < (int)slots_.size(); s++)
+        if (!slots_[s].used) {
+            slot = s;
+            break;
+        }
+    if (slot < 0) {
+        if ((int)slots_.size() >= max_domains_)
+            throw std::runtime_error("admission refused: too many domains");
+        slot = (int)slots_.size();
+        slots_.emplace_back();
+        host_desc_.emplace_back();
+    }
+    SlotHost &s = slots_[slot];
+    s = SlotHost();
+    s.used = true;
+    s.problem = pp;
+    const Geometry &g = p.g;
+    size_t N = g.domain_size, A = g.active_size;
+    DomainDesc d;
+    std::memset(&d, 0, sizeof(d));
+    d.ctype = dalloc<int8_t>(N, s.allocs, s.bytes);
+    d.gid = dalloc<int32_t>(N, s.allocs, s.bytes);
+    d.cts = dalloc<int32_t>(N, s.allocs, s.bytes);
+    d.layer = dalloc<int8_t>(N, s.allocs, s.bytes);
+    d.du = dalloc<float>(N, s.allocs, s.bytes);
+    d.dl = dalloc<float>(A, s.allocs, s.bytes);
+    d.doc = dalloc<float>(3 * A, s.allocs, s.bytes);
+    d.cdl = dalloc<float>(26 * A, s.allocs, s.bytes);
+    d.claim = dalloc<unsigned long long>(A, s.allocs, s.bytes);
+    // nuclei in time order; ties keep the reference's order (order does not change results)
+    size_t P = p.nuclei_loc.size();
+    std::vector<int> order(P);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return p.nuclei_time[a] < p.nuclei_time[b]; });
+    std::vector<int32_t> nl(P), nt(P);
+    for (size_t q = 0; q < P; q++) {
+        nl[q] = p.nuclei_loc[order[q]];
+        nt[q] = p.nuclei_time[order[q]];
+    }
+    int32_t *dnl = dalloc<int32_t>(P, s.allocs, s.bytes);
+    int32_t *dnt = dalloc<int32_t>(P, s.allocs, s.bytes);
+    cudaStream_t st = S(stream_);
+    CUDA_OK(cudaMemcpyAsync(d.ctype, p.cell_type.data(), N, cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d.gid, p.grain_id.data(), N * 4, cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d.cts, p.cts.data(), N * 4, cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d.layer, p.layer_id.data(), N, cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemcpyAsync(d.du, p.du.data(), N * 4, cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaMemsetAsync(d.dl, 0, A * 4, st));
+    CUDA_OK(cudaMemsetAsync(d.claim, 0xff, A * 8, st));
+    if (P) {
+        CUDA_OK(cudaMemcpyAsync(dnl, nl.data(), P * 4, cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(dnt, nt.data(), P * 4, cudaMemcpyHostToDevice, st));
+    }
+    const DeviceTables &tb = tables_for(p);
+    d.guv = tb.guv;
+    d.cdl_table = tb.cdl_table;
+    d.nuc_loc = dnl;
+    d.nuc_time = dnt;
+    d.n_nuclei = (int)P;
+    d.mx = g.mx;
+    d.my = g.my;
+    d.nz = g.nz;
+    d.nz_active = g.nz_active;
+    d.xoff = g.xoff;
+    d.yoff = g.yoff;
+    d.zbound_high = g.zbound_high;
+    d.check_mode = check_mode;
+    d.domain_size = g.domain_size;
+    d.active_size = g.active_size;
+    d.du_value = p.du_value;
+    long long liquid = 0;
+    for (long i = 0; i < g.domain_size; i++)
+        if (p.cell_type[i] == kLiquid && p.layer_id[i] == 0)
+            liquid++;
+    d.liquid = liquid;
+    host_desc_[slot] = d;
+    push_desc(slot);
+    ensure_growth(slot, 4096);
+    if (!p.voronoi_seeds.empty() || p.cfg.simulation_type == "S") {
+        int nseeds = (int)(p.voronoi_seeds.size() / 3);
+        int32_t *dseeds = nullptr;
+        if (nseeds) {
+            CUDA_OK(cudaMalloc(&dseeds, p.voronoi_seeds.size() * 4));
+            CUDA_OK(cudaMemcpyAsync(dseeds, p.voronoi_seeds.data(), p.voronoi_seeds.size() * 4,
+                                    cudaMemcpyHostToDevice, st));
+        }
+        long long blocks = (g.domain_size + 255) / 256;
+        k_voronoi<<<(unsigned)blocks, 256, 3 * 1024 * sizeof(int), st>>>(ddesc_ + slot, dseeds, nseeds,
+                                                                         (float)(g.active_size));
+        CUDA_OK(cudaGetLastError());
+        CUDA_OK(cudaStreamSynchronize(st));
+        if (dseeds)
+            CUDA_OK(cudaFree(dseeds));
+    }
+    // register the domain, then build its initial active list in the list the next cycle consumes
+    PoolState ps;
+    CUDA_OK(cudaMemcpyAsync(&ps, dstate_, sizeof(ps), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    int n_domains = std::max(ps.n_domains, slot + 1);
+    CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, n_domains), &n_domains, sizeof(int),
+                            cudaMemcpyHostToDevice, st));
+    int next_slot = ps.cur ^ 1;
+    k_init_active<<<num_sms_ * 4, 256, 0, st>>>(dstate_, slot, next_slot);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaStreamSynchronize(st));
+    bytes_in_use_ += s.bytes;
+    return slot;
+}
+
+void Pool::retire(int slot) {
+    CUDA_OK(cudaSetDevice(device_));
+    SlotHost &s = slots_.at(slot);
+    if (!s.used)
+        return;
+    cudaStream_t st = S(stream_);
+    // mark done and drop its list entries before the memory goes away
+    int one = 1;
+    CUDA_OK(cudaMemcpyAsync((char *)(ddesc_ + slot) + offsetof(DomainDesc, done), &one, sizeof(int),
+                            cudaMemcpyHostToDevice, st));
+    k_drop_domain<<<num_sms_ * 2, 256, 0, st>>>(dstate_, (unsigned)slot, (unsigned)max_domains_);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaStreamSynchronize(st));
+    DomainDesc zero;
+    std::memset(&zero, 0, sizeof(zero));
+    zero.done = 1;
+    host_desc_[slot] = zero;
+    CUDA_OK(cudaMemcpyAsync(ddesc_ + slot, &zero, sizeof(zero), cudaMemcpyHostToDevice, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    for (void *p : s.allocs)
+        CUDA_OK(cudaFree(p));
+    if (s.growth)
+        CUDA_OK(cudaFree(s.growth));
+    bytes_in_use_ -= s.bytes;
+    s = SlotHost();
+}
+
+void Pool::launch_step() {
+    cudaStream_t st = S(stream_);
+    k_step_begin<<<1, 512, 0, st>>>(dstate_);
+    k_grow_claim<<<num_sms_ * 8, 256, 0, st>>>(dstate_);
+    k_capture<<<num_sms_ * 8, 256, 0, st>>>(dstate_);
+}
+
+void Pool::build_graph() {
+    if (graph_exec_)
+        return;
+    graph_steps_ = 50;
+    cudaStream_t st = S(stream_);
+    cudaGraph_t graph;
+    CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    for (int q = 0; q < graph_steps_; q++)
+        launch_step();
+    CUDA_OK(cudaStreamEndCapture(st, &graph));
+    cudaGraphExec_t ex;
+    CUDA_OK(cudaGraphInstantiate(&ex, graph, 0));
+    CUDA_OK(cudaGraphDestroy(graph));
+    graph_exec_ = ex;
+}
+
+void Pool::step(int n) {
+    if (n <= 0)
+        return;
+    CUDA_OK(cudaSetDevice(device_));
+    for (int s = 0; s < (int)slots_.size(); s++) {
+        if (!slots_[s].used)
+            continue;
+        slots_[s].steps_launched += n;
+        ensure_growth(s, slots_[s].steps_launched + 1);
+    }
+    build_graph();
+    cudaStream_t st = S(stream_);
+    int full = n / graph_steps_, rest = n % graph_steps_;
+    for (int q = 0; q < full; q++)
+        CUDA_OK(cudaGraphLaunch((cudaGraphExec_t)graph_exec_, st));
+    for (int q = 0; q < rest; q++)
+        launch_step();
+    CUDA_OK(cudaGetLastError());
+}
+
+void Pool::sync_state() {
+    CUDA_OK(cudaSetDevice(device_));
+    cudaStream_t st = S(stream_);
+    if (!host_desc_.empty())
+        CUDA_OK(cudaMemcpyAsync(host_desc_.data(), ddesc_, sizeof(DomainDesc) * host_desc_.size(),
+                                cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+}
+
+int Pool::pool_error() {
+    int e = 0;
+    CUDA_OK(cudaMemcpyAsync(&e, (char *)dstate_ + offsetof(PoolState, error), sizeof(int), cudaMemcpyDeviceToHost,
+                            S(stream_)));
+    CUDA_OK(cudaStreamSynchronize(S(stream_)));
+    return e;
+}
+
+unsigned long long Pool::list_count() {
+    PoolState ps;
+    CUDA_OK(cudaMemcpyAsync(&ps, dstate_, sizeof(ps), cudaMemcpyDeviceToHost, S(stream_)));
+    CUDA_OK(cudaStreamSynchronize(S(stream_)));
+    return ps.cnt[ps.cur ^ 1];
+}
+
+Census Pool::census(int slot) {
+    CUDA_OK(cudaSetDevice(device_));
+    cudaStream_t st = S(stream_);
+    Census init;
+    std::memset(&init, 0, sizeof(init));
+    init.next_cts = ULLONG_MAX;
+    CUDA_OK(cudaMemcpyAsync(census_buf_, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+    k_census<<<num_sms_ * 4, 256, 0, st>>>(ddesc_ + slot, (Census *)census_buf_);
+    CUDA_OK(cudaGetLastError());
+    Census out;
+    CUDA_OK(cudaMemcpyAsync(&out, census_buf_, sizeof(out), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    return out;
+}
+
+void Pool::set_cycle(int slot, int cycle) {
+    sync_state();
+    DomainDesc &h = host_desc_[slot];
+    if (cycle > h.cycle) {
+        if (h.n_jumps >= kMaxJumps)
+            throw std::runtime_error("too many cycle jumps");
+        h.jump_lo[h.n_jumps] = h.cycle;
+        h.jump_hi[h.n_jumps] = cycle;
+        h.n_jumps++;
+    }
+    h.cycle = cycle;
+    // only this slot's dynamic fields change; nothing else is in flight on the stream
+    push_desc(slot);
+}
+
+void Pool::copy_out_raw(int slot, int32_t *grain_id, int8_t *cell_type) {
+    CUDA_OK(cudaSetDevice(device_));
+    const DomainDesc &d = host_desc_.at(slot);
+    size_t N = slots_.at(slot).problem->g.domain_size;
+    cudaStream_t st = S(stream_);
+    if (grain_id)
+        CUDA_OK(cudaMemcpyAsync(grain_id, d.gid, N * 4, cudaMemcpyDeviceToHost, st));
+    if (cell_type)
+        CUDA_OK(cudaMemcpyAsync(cell_type, d.ctype, N, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+}
+
+void Pool::copy_octahedra(int slot, float *dl, float *doc, float *cdl) {
+    CUDA_OK(cudaSetDevice(device_));
+    const DomainDesc &d = host_desc_.at(slot);
+    size_t A = slots_.at(slot).problem->g.active_size;
+    cudaStream_t st = S(stream_);
+    if (dl)
+        CUDA_OK(cudaMemcpyAsync(dl, d.dl, A * 4, cudaMemcpyDeviceToHost, st));
+    if (doc)
+        CUDA_OK(cudaMemcpyAsync(doc, d.doc, A * 12, cudaMemcpyDeviceToHost, st));
+    if (cdl)
+        CUDA_OK(cudaMemcpyAsync(cdl, d.cdl, A * 104, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+}
+
+void Pool::copy_out(int slot, int32_t *grain_id, int32_t *cell_type) {
+    size_t N = slots_.at(slot).problem->g.domain_size;
+    std::vector<int8_t> ct;
+    if (cell_type)
+        ct.resize(N);
+    copy_out_raw(slot, grain_id, cell_type ? ct.data() : nullptr);
+    if (cell_type)
+        for (size_t i = 0; i < N; i++)
+            cell_type[i] = ct[i];
+}
+
+int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_s) {
+    // src/runCA.cpp:283-342 for one layer
+    const Problem &p = *slots_.at(slot).problem;
+    bool jump_type = p.cfg.simulation_type == "S" || p.cfg.simulation_type == "R";
+    auto t0 = std::chrono::steady_clock::now();
+    sync_state();
+    int cycle = host_desc_[slot].cycle;
+    while (true) {
+        int n = 1000 - (cycle % 1000);
+        step(n);
+        sync_state();
+        const DomainDesc &d = host_desc_[slot];
+        int perr = pool_error();
+        if (d.error || perr) {
+            std::ostringstream e;
+            e << "device error flags: domain " << d.error << " pool " << perr;
+            throw std::runtime_error(e.str());
+        }
+        cycle = d.cycle;
+        Census c = census(slot);
+        std::ostringstream s;
+        s << "cycle = " << cycle << " Superheated liquid cells = " << c.superheated
+          << " Undercooled liquid cells = " << c.undercooled << " Number of nucleation events this layer " << d.nn
+          << " Remaining liquid cells in future layers of this simulation = " << c.remaining << "\n";
+        log += s.str();
+        if (c.superheated + c.undercooled == 0)
+            break;
+        if (jump_type && c.undercooled == 0) {
+            unsigned long long next = c.next_cts;
+            if ((next - (unsigned long long)(long long)cycle) > 5000) {
+                int nc = (int)(next - 1);
+                set_cycle(slot, nc);
+                cycle = nc;
+                log += "Jumping to cycle " + std::to_string(cycle + 1) + "\n";
+            }
+        }
+    }
+    double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    if (nucl_s)
+        *nucl_s = 0.0;
+    if (capture_s)
+        *capture_s = secs;
+    slots_[slot].finished = true;
+    return cycle;
+}
+
+} // namespace exaca

@@ -1,0 +1,152 @@
+// Host-side data model of one ExaCA problem (one domain) for the B200 solver.
+//
+// The reference keeps this state in ~20 Kokkos views owned by RunProgram_Reduced
+// (src/runCA.cpp:19-256). Here it is one Problem object: parsed inputs, the single-rank geometry,
+// and the initialised fields that are uploaded once to a device pool slot.
+#pragma once
+
+#include <cstdint>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace exaca {
+
+// Cell types, same numbering as the reference enum TypeNames (src/CAtypes.hpp:11).
+enum CellTypeCode : int8_t {
+    kWall = 0,
+    kSolid = 1,
+    kActive = 2,
+    kTemporaryUpdate = 3,
+    kTemporaryInit = 4,
+    kLiquid = 5,
+    kGhost = 6
+};
+
+constexpr int kNumOrientations = 10000; // src/runCA.cpp:133
+
+// Every value the reference reads from an input file and its material file
+// (src/CAinitialize.cpp:232-576). Units follow the reference: deltax and deltat in SI.
+struct InputConfig {
+    std::string input_file;
+    std::string simulation_type; // "C", "S" or "R"
+    int decomposition_strategy = 1;
+    std::string material_name;
+    double A = 0, B = 0, C = 0, D = 0, freezing_range = 0;
+    double deltax = 0;  // m
+    double nread = 0;   // nucleation density / 1e12
+    double nmax = 0;    // m^-3
+    double dTN = 0, dTsigma = 0;
+    std::string path_to_output, output_file;
+    std::string orientation_file; // resolved path
+    // type R (parsed for error parity; the solver rejects R)
+    double ht_deltax = 0;
+    std::string temppath, tempfile;
+    int temp_files_in_series = 0;
+    bool extra_walls = false;
+    bool remelting = false;
+    // time step and layers
+    double deltat = 0;
+    int number_of_layers = 1, layer_height = 0;
+    // substrate (S/R)
+    std::string substrate_file_name;
+    float substrate_grain_spacing = 0.0f;
+    bool use_substrate_file = false;
+    // C and S
+    double G = 0, R = 0;
+    int nx = 0, ny = 0, nz = 0;
+    double fract_surface_sites_active = 0;
+    int nspots_x = 0, nspots_y = 0, spot_offset = 0, spot_radius = 0;
+    // outputs
+    int print_debug = 0;
+    bool print_misorientation = false, print_full_output = false;
+};
+
+// Single-rank decomposition (src/CAfunctions.cpp:34-166 at np = 1): one ghost/wall ring in x and y.
+struct Geometry {
+    int nx = 0, ny = 0, nz = 0; // global sizes, wall layers included
+    int mx = 0, my = 0;         // MyXSlices, MyYSlices
+    int xoff = 0, yoff = 0;     // MyXOffset, MyYOffset
+    int nz_active = 0, zbound_low = 0, zbound_high = 0;
+    long domain_size = 0; // mx * my * nz
+    long active_size = 0; // mx * my * nz_active
+    int procs_x = 1, procs_y = 1;
+};
+
+// A fully initialised problem, ready to be admitted to a device pool.
+struct Problem {
+    InputConfig cfg;
+    Geometry g;
+    // per-cell fields over the whole domain (index k*mx*my + i*my + j, y fastest)
+    std::vector<int32_t> cts;      // CritTimeStep
+    std::vector<int8_t> layer_id;  // LayerID (single layer: -1 or 0)
+    std::vector<float> du;         // UndercoolingChange
+    std::vector<int8_t> cell_type; // CellType
+    std::vector<int32_t> grain_id; // GrainID
+    std::vector<uint8_t> melted;   // Melted
+    // orientation table: 9 floats per orientation (src/CAinitialize.cpp:1408-1441)
+    std::vector<float> guv;
+    // fresh-octahedron critical diagonal lengths, 26 per orientation
+    std::vector<float> cdl_table;
+    // potential nuclei in the reference's order (src/CAinitialize.cpp:2240-2247)
+    std::vector<int32_t> nuclei_loc, nuclei_time;
+    // interfacial response constants after the dt/dx normalisation of src/runCA.cpp:198-200
+    double A_n = 0, B_n = 0, C_n = 0, D_n = 0;
+    float du_value = 0.0f; // the one non-zero UndercoolingChange value of this problem
+    int possible_nuclei = 0;
+    double init_seconds = 0.0;
+    // baseplate grain centres (x, y, z triples) for the device Voronoi pass of S problems
+    std::vector<int32_t> voronoi_seeds;
+};
+
+// GrainID placeholder for substrate cells whose Voronoi assignment is computed on the device.
+constexpr int32_t kVoronoiPending = INT32_MIN;
+
+// Parses an ExaCA input file (and its material file); throws std::runtime_error with the
+// reference's messages on malformed input. `log` receives the reference's rank-0 stdout lines.
+void read_input_file(const std::string &path, InputConfig &cfg, std::string &log);
+
+// Locates a data file the way checkFileInstalled does (src/CAinitialize.cpp:217-229): the
+// install directory first, then the source data directory. Here: $EXACA_DATA_DIR, then the
+// package's data directory.
+std::string find_data_file(const std::string &name, const std::string &type, std::string &log);
+
+// Builds the geometry, temperature field, substrate, grains and nuclei of a C or S problem
+// (src/CAinitialize.cpp:579-2769). Throws for unsupported problem kinds.
+void initialize_problem(Problem &p, std::string &log);
+
+// Host tables derived from the orientation file.
+void read_orientations(const std::string &path, std::vector<float> &guv);
+void build_cdl_table(const std::vector<float> &guv, std::vector<float> &table);
+
+// Output writers (src/CAprint.cpp:170-571), byte-compatible with the reference.
+void write_vtk_fields(const Problem &p, const int32_t *grain_id, const std::string &fname);
+void write_misorientations(const Problem &p, const int32_t *grain_id, const std::string &fname,
+                           std::string &log);
+void write_debug_vtk(const Problem &p, const std::string &fname);
+
+struct RunTimes {
+    double init = 0, run = 0, out = 0, nucl = 0, capture = 0, ghost = 0;
+};
+void write_log(const Problem &p, const std::string &fname, int cycle, const RunTimes &t, std::string &out);
+
+// neighbour offsets in the reference's order (src/CAinitialize.cpp:595-674)
+extern const int kNeighborX[26];
+extern const int kNeighborY[26];
+extern const int kNeighborZ[26];
+// ItList(9,26) and the per-case list lengths (src/CAinitialize.cpp:676-745)
+void build_itlist(int itlist[9][26], int lens[9]);
+inline int find_it_bounds(int rx, int ry, int mx, int my) {
+    // src/CAfunctions.cpp:169-213
+    if (ry == 0)
+        return rx == 0 ? 5 : (rx == mx - 1 ? 6 : 1);
+    if (ry == my - 1)
+        return rx == 0 ? 7 : (rx == mx - 1 ? 8 : 2);
+    return rx == 0 ? 3 : (rx == mx - 1 ? 4 : 0);
+}
+
+// Growth-increment table: entry n is the diagonal-length increment of an active cell whose
+// undercooling is the n-fold float sum of du (src/CAupdate.cpp:236-261). Entry 0 is U = 0.
+void build_growth_table(const Problem &p, int n_entries, std::vector<double> &growth);
+
+} // namespace exaca

@@ -1,0 +1,156 @@
+// Device pool of ExaCA domains: the B200 runtime behind the C ABI.
+//
+// A pool owns a set of independent domains (one for the plain solver, hundreds for batched or
+// served process maps). Every domain's fields live in their own HBM allocations; all domains share
+// one compacted active-cell list, so one launch of each step kernel advances every admitted domain
+// by one CA cycle. The step loop is replayed as a captured CUDA graph.
+#pragma once
+
+#include <cstdint>
+#include <map>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "exaca_host.hpp"
+
+namespace exaca {
+
+constexpr int kMaxJumps = 32;
+
+// Device-resident descriptor of one domain. Static fields are written at admission; dynamic
+// fields are advanced by the step kernels and read back by the host.
+struct DomainDesc {
+    // fields (index k*mx*my + i*my + j; the active window starts at k = 0 for single-layer problems)
+    int8_t *ctype;
+    int32_t *gid;
+    int32_t *cts;
+    int8_t *layer;
+    float *du;
+    float *dl;
+    float *doc;               // 3 per active-window cell
+    float *cdl;               // 26 per active-window cell
+    unsigned long long *claim; // per active-window cell: (~epoch << 32) | capturer index
+    const double *growth;     // growth increment by number of undercooling updates
+    const float *guv;         // 9 per orientation
+    const float *cdl_table;   // 26 per orientation
+    const int32_t *nuc_loc;   // nuclei sorted by nucleation time
+    const int32_t *nuc_time;
+    int growth_len;
+    int n_nuclei;
+    int mx, my, nz, nz_active, xoff, yoff, zbound_high;
+    int check_mode; // 1: the device ends the domain at cycle % 1000 == 0 once no liquid is left
+    long long domain_size, active_size;
+    float du_value;
+    int pad0;
+    // dynamic state
+    int cycle;
+    unsigned int epoch;
+    int nuc_cursor;
+    int done;
+    int nn;
+    int error;
+    long long liquid;
+    int n_jumps;
+    int jump_lo[kMaxJumps];
+    int jump_hi[kMaxJumps];
+    unsigned long long n_grown;    // eligible active-cell updates executed
+    unsigned long long n_captured; // captures executed
+    unsigned long long n_listed;   // list entries visited
+};
+
+// Pool-level device state.
+struct PoolState {
+    unsigned long long *list[2]; // entries: (domain << 32) | cell
+    unsigned int *mask;          // per entry of the current list
+    unsigned long long cnt[2];
+    unsigned long long capacity;
+    int cur;
+    int error;
+    int n_domains;
+    int pad;
+    DomainDesc *desc;
+};
+
+// Result of the reference's every-1000-cycle census (src/CAupdate.cpp:738-808).
+struct Census {
+    unsigned long long superheated, undercooled, active, solid, remaining;
+    unsigned long long next_cts; // min CritTimeStep of liquid cells in the active window
+};
+
+struct DeviceTables {
+    float *guv = nullptr;
+    float *cdl_table = nullptr;
+};
+
+struct SlotHost {
+    bool used = false;
+    std::shared_ptr<const Problem> problem;
+    std::vector<void *> allocs;
+    double *growth = nullptr;
+    int growth_len = 0;
+    long long steps_launched = 0; // upper bound on executed updates of any cell of the slot
+    size_t bytes = 0;
+    int n_jumps = 0;
+    bool finished = false;
+};
+
+class Pool {
+  public:
+    Pool(int device, size_t budget_bytes, unsigned long long list_capacity);
+    ~Pool();
+    Pool(const Pool &) = delete;
+    Pool &operator=(const Pool &) = delete;
+
+    // HBM bytes a problem needs in a pool slot.
+    static size_t slot_bytes(const Problem &p);
+    // Uploads an initialised problem; returns the slot index. check_mode 1 lets the device end
+    // the domain on its own; 0 leaves termination to run_plain's host-side census.
+    int admit(std::shared_ptr<const Problem> p, int check_mode);
+    void retire(int slot);
+    // Advances every unfinished domain by n cycles (graph replay).
+    void step(int n);
+    // Reads back the dynamic state of all slots.
+    void sync_state();
+    const DomainDesc &state(int slot) const { return host_desc_.at(slot); }
+    Census census(int slot);
+    void copy_out(int slot, int32_t *grain_id, int32_t *cell_type);
+    void copy_out_raw(int slot, int32_t *grain_id, int8_t *cell_type);
+    void copy_octahedra(int slot, float *dl, float *doc, float *cdl);
+    // Reference-equivalent run of one slot to completion with the reference's 1000-cycle census,
+    // stdout progress lines and type-S cycle jumps (src/runCA.cpp:290-342).
+    int run_plain(int slot, std::string &log, double *nucl_s, double *capture_s);
+    int n_slots() const { return (int)slots_.size(); }
+    bool slot_used(int s) const { return s < (int)slots_.size() && slots_[s].used; }
+    size_t bytes_in_use() const { return bytes_in_use_; }
+    size_t budget() const { return budget_; }
+    int device() const { return device_; }
+    unsigned long long list_count();
+    void set_cycle(int slot, int cycle);
+    int pool_error();
+
+  private:
+    void ensure_growth(int slot, long long needed);
+    void push_desc(int slot);
+    void launch_step();
+    void build_graph();
+    const DeviceTables &tables_for(const Problem &p);
+
+    int device_;
+    size_t budget_;
+    size_t bytes_in_use_ = 0;
+    void *stream_ = nullptr; // cudaStream_t
+    void *graph_exec_ = nullptr;
+    int graph_steps_ = 0;
+    PoolState *dstate_ = nullptr;
+    DomainDesc *ddesc_ = nullptr;
+    int max_domains_ = 0;
+    unsigned long long capacity_ = 0;
+    std::vector<SlotHost> slots_;
+    std::vector<DomainDesc> host_desc_;
+    std::map<std::string, DeviceTables> tables_;
+    int num_sms_ = 148;
+    void *census_buf_ = nullptr;
+};
+
+} // namespace exaca

@@ -1,0 +1,130 @@
+/*
+ * C ABI of the B200-native ExaCA cellular-automaton solver (libexaca_b200.so).
+ *
+ * The reference (ExaCA, Kokkos + MPI) exposes no plugin or FFI layer: its boundary is the
+ * ExaCA-Kokkos executable, the driver RunProgram_Reduced and the three step functions. Every entry
+ * point below names the reference interface it replaces. All functions return 0 on success and a
+ * negative error code otherwise (never throw across the ABI); exaca_last_error() returns the
+ * message of the last failure on the calling thread. Pointers are plain host pointers; the library
+ * owns all device memory. One pool is driven by one host thread at a time; separate pools may be
+ * used from separate threads.
+ */
+#ifndef EXACA_B200_H
+#define EXACA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define EXACA_OK 0
+#define EXACA_ERR_INPUT (-1)     /* malformed input file, missing key or data file */
+#define EXACA_ERR_UNSUPPORTED (-2) /* a problem kind this solver does not handle (type R, >1 layer) */
+#define EXACA_ERR_CUDA (-3)      /* CUDA runtime failure or device-side error flag */
+#define EXACA_ERR_BUDGET (-4)    /* admission refused: HBM budget or slot limit */
+#define EXACA_ERR_ARG (-5)       /* bad handle, slot or size */
+
+typedef struct exaca_problem exaca_problem; /* parsed and initialised host-side problem */
+typedef struct exaca_pool exaca_pool;       /* device pool of domains */
+
+/* Geometry of a problem (src/CAfunctions.cpp:34-166 at one rank). */
+typedef struct {
+    int nx, ny, nz;        /* global sizes including the wall layers */
+    int mx, my;            /* MyXSlices, MyYSlices (nx + 2, ny + 2) */
+    int nz_active;         /* active window height */
+    int64_t domain_size;   /* mx * my * nz cells, index k*mx*my + i*my + j */
+    int64_t active_size;   /* mx * my * nz_active */
+    int n_nuclei;          /* potential nucleation sites */
+    double deltat;         /* s */
+    char simulation_type;  /* 'C' or 'S' */
+} exaca_problem_geometry;
+
+/* Parameters of a synthetic directional-solidification problem, equal to an input file of
+ * problem type C with these values (keys of src/CAinitialize.cpp:395-441). */
+typedef struct {
+    int nx, ny, nz;                  /* "Domain size in x/y/z" (cells, without walls) */
+    double cell_size_um;             /* "Cell size" */
+    double G, R;                     /* "Thermal gradient" K/m, "Cooling rate" K/s */
+    int n_ratio;                     /* "N": deltat = deltax / (N * R / G) */
+    double nucleation_density;       /* "Heterogeneous nucleation density" (x 1e12 m^-3) */
+    double dTN, dTsigma;             /* mean / sigma of the nucleation undercooling (K) */
+    double fract_surface_active;     /* "Fraction of surface sites active" */
+    double A, B, C, D, freezing_range; /* material file values */
+} exaca_dirs_params;
+
+/* Dynamic state of one pool slot. */
+typedef struct {
+    int cycle;          /* last executed CA cycle */
+    int done;           /* 1 once the domain met the reference's termination test */
+    int nn;             /* nucleation events so far */
+    int error;          /* device error flags (0 = none) */
+    int64_t liquid;     /* liquid cells left */
+    uint64_t n_grown;   /* active-cell growth updates executed */
+    uint64_t n_captured;/* captures executed */
+    uint64_t n_listed;  /* active-list entries visited */
+} exaca_domain_status;
+
+/* The reference's every-1000-cycle census (src/CAupdate.cpp:738-808). */
+typedef struct {
+    uint64_t superheated, undercooled, active, solid, remaining, next_cts;
+} exaca_census;
+
+const char *exaca_last_error(void);
+
+/* Drop-in for RunProgram_Reduced(int id, int np, std::string InputFile) (src/runCA.hpp:11) and the
+ * ExaCA-Kokkos main (src/main.cpp:15-47) at np = 1: reads the input file, initialises, solves on
+ * CUDA device `device`, writes the .vtk / _Misorientations.vtk / .log outputs and prints the
+ * reference's progress lines to stdout. */
+int exaca_run_program(const char *input_file, int device);
+
+/* Input parsing and initialisation: InputReadFromFile + ParallelMeshInit + TempInit_* +
+ * OrientationInit + SubstrateInit_* + ActiveCellWallInit + GrainInit + NucleiInit
+ * (src/CAinitialize.hpp:16-96; src/runCA.cpp:38-195). Host only; no device needed. */
+int exaca_problem_from_file(const char *input_file, exaca_problem **out);
+int exaca_problem_directional(const exaca_dirs_params *prm, exaca_problem **out);
+void exaca_problem_free(exaca_problem *p);
+int exaca_problem_info(const exaca_problem *p, exaca_problem_geometry *info);
+/* Initial fields (domain_size values each; any pointer may be NULL). GrainID entries of
+ * Voronoi-baseplate cells read INT32_MIN here; the device fills them in at admission. */
+int exaca_problem_fields(const exaca_problem *p, int32_t *cell_type, int32_t *grain_id, int32_t *crit_time_step,
+                         float *undercooling_change, int32_t *layer_id);
+/* Bytes of HBM a problem takes in a pool slot. */
+int64_t exaca_problem_slot_bytes(const exaca_problem *p);
+
+/* Device pool: replaces the device-side views of src/runCA.cpp:232-256. budget_bytes bounds the
+ * per-slot allocations (admission control); list_capacity sizes the shared active-cell list. */
+int exaca_pool_create(int device, size_t budget_bytes, uint64_t list_capacity, exaca_pool **out);
+void exaca_pool_destroy(exaca_pool *pool);
+/* Uploads a problem (the host->device mirror copies of src/runCA.cpp:234-250) and finishes its
+ * initialisation on the device. device_check = 1 lets the device end the domain at the
+ * reference's termination test; 0 leaves it to exaca_pool_run_plain. */
+int exaca_pool_admit(exaca_pool *pool, const exaca_problem *p, int device_check, int *slot);
+/* Advances every unfinished domain by n_cycles CA cycles: Nucleation + CellCapture
+ * (src/CAupdate.hpp:15-29) per cycle, replayed as a CUDA graph. Asynchronous. */
+int exaca_pool_step(exaca_pool *pool, int n_cycles);
+/* Waits for the device and reads one slot's state. */
+int exaca_pool_status(exaca_pool *pool, int slot, exaca_domain_status *st);
+/* IntermediateOutputAndCheck's census (src/CAupdate.hpp:30-33) for one slot. */
+int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c);
+/* Runs one slot to completion exactly as the reference's layer loop (src/runCA.cpp:290-342):
+ * 1000-cycle census, termination, type-S cycle jump; progress lines are appended to stdout when
+ * verbose is 1. */
+int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cycle);
+/* Device->host copy of GrainID and CellType (src/runCA.cpp:423-424); NULL skips a field. */
+int exaca_pool_copy_out(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *cell_type);
+/* Active-window octahedron state (DiagonalLength, DOCenter x3, CritDiagonalLength x26). */
+int exaca_pool_copy_octahedra(exaca_pool *pool, int slot, float *dl, float *doc, float *cdl);
+/* Frees a slot's device memory. */
+int exaca_pool_retire(exaca_pool *pool, int slot);
+int64_t exaca_pool_bytes_in_use(exaca_pool *pool);
+
+/* Writes the reference's output files for a finished slot (src/CAprint.cpp:170-571). */
+int exaca_pool_write_outputs(exaca_pool *pool, int slot, const exaca_problem *p, const char *path_prefix);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

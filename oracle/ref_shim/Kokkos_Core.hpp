@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cstddef>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <iostream>
@@ -52,9 +53,32 @@ template <class T> struct rank_of<T *> {
     static constexpr int value = 1 + rank_of<T>::value;
     using value_type = typename rank_of<T>::value_type;
 };
+// With EXACA_SHIM_DUMP_DIR set, the storage of the views named below is written to
+// $EXACA_SHIM_DUMP_DIR/<label>.bin when it is released, i.e. the reference's final state at the
+// end of RunProgram_Reduced. Used to build golden arrays; the reference code is not touched.
+inline bool dump_label(const std::string &l) {
+    static const char *names[] = {"GrainID", "CellType", "DiagonalLength", "DOCenter", "CritDiagonalLength",
+                                  "UndercoolingCurrent", "CritTimeStep", "UndercoolingChange", "LayerID"};
+    for (const char *n : names)
+        if (l == n)
+            return true;
+    return false;
+}
 struct Storage {
     void *ptr = nullptr;
-    ~Storage() { std::free(ptr); }
+    size_t bytes = 0;
+    std::string label;
+    ~Storage() {
+        const char *dir = std::getenv("EXACA_SHIM_DUMP_DIR");
+        if (dir && ptr && dump_label(label)) {
+            std::string f = std::string(dir) + "/" + label + ".bin";
+            if (FILE *fp = std::fopen(f.c_str(), "wb")) {
+                std::fwrite(ptr, 1, bytes, fp);
+                std::fclose(fp);
+            }
+        }
+        std::free(ptr);
+    }
 };
 } // namespace shim_detail
 
@@ -112,6 +136,8 @@ template <class DataType, class... Props> class View {
         size_t n = size();
         store_ = std::make_shared<shim_detail::Storage>();
         store_->ptr = std::calloc(n == 0 ? 1 : n, sizeof(value_type));
+        store_->bytes = n * sizeof(value_type);
+        store_->label = label;
         if (!store_->ptr)
             throw std::runtime_error("shim View allocation failed: " + label);
         data_ = static_cast<value_type *>(store_->ptr);

@@ -1,0 +1,50 @@
+"""Shared helpers of the parity tests (test infrastructure)."""
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+GOLDEN = os.path.join(HERE, "golden")
+INPUTS = os.path.join(GOLDEN, "inputs")
+
+
+def golden_cases():
+    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+
+
+def load_golden(case):
+    return np.load(os.path.join(GOLDEN, case + ".npz"))
+
+
+def input_path(case):
+    return os.path.join(INPUTS, case + ".txt")
+
+
+def to_whole(a, shape):
+    """Rank-local array (nz, mx, my) -> the reference's whole-domain print grid (nz, ny, nx),
+    ghost ring dropped, planes k = 0 and nz - 1 zeroed (src/CAprint.cpp:18-29, 285-346)."""
+    nz, mx, my = shape
+    w = a.reshape(nz, mx, my)[:, 1:-1, 1:-1].transpose(0, 2, 1).copy()
+    w[0] = 0
+    w[-1] = 0
+    return w
+
+
+def copy_input(case, outdir):
+    """Copy of an input file whose outputs go to outdir."""
+    lines = open(input_path(case)).read().splitlines()
+    out = []
+    for ln in lines:
+        if ln.startswith("Path to output"):
+            ln = "Path to output: " + outdir + "/"
+        out.append(ln)
+    dst = os.path.join(outdir, case + ".txt")
+    open(dst, "w").write("\n".join(out) + "\n")
+    return dst
+
+
+def output_base(case):
+    for ln in open(input_path(case)):
+        if ln.startswith("Output file base name"):
+            return ln.split(":", 1)[1].strip()
+    raise KeyError(case)
