@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 ExaCA solver on the 512^3 directional-solidification case.
+
+Workload (one "step" = one complete solve, initial state -> termination): problem type C,
+512 x 512 x 512 cells of 1 um (516 x 516 x 514 allocated with the wall ring), G = 1e6 K/m,
+R = 1e6 K/s, N = 25 (dt = 0.04 us), Inconel625 interfacial response, 2 % of the bottom surface
+seeded, bulk nucleation density 1e14 m^-3 with undercooling N(3 K, 0.5 K). Synthetic inputs: the
+problem is generated from those parameters by the solver's own initialisation (seeded exactly as
+the reference seeds it).
+
+metric: cell-updates/s = active-window cells x CA cycles executed / solve time (the reference's
+per-cycle sweep size times cycles). `value` is timed with CUDA events around each solve with the
+initial state already resident in HBM; `e2e` times the same solve through the C ABI from pinned host
+buffers (admission upload + solve + GrainID/CellType download). The state (~20 GB) is larger than
+L2 and is re-uploaded between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size S]
+
+For N > 1 (torchrun) every rank solves its own replica (the plain path has no exchange step) and
+rank 0 prints the aggregate over ranks with the max-over-ranks time.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "cell-updates/s"
+UNIT = "cell-updates/s"
+WORKLOAD = dict(G=1e6, R=1e6, n_ratio=25, nucleation_density=100.0, dTN=3.0, dTsigma=0.5, fract_surface_active=0.02)
+REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+
+# algorithmic bytes per unit of work of the two step kernels ("Roofline")
+GROW_BYTES = dict(listed=12, grown=142, claims=8)
+CAPTURE_BYTES = dict(listed=12, kept=8, liquid_nb=8, captured=185)
+
+
+def input_file_text(n):
+    return "\n".join([
+        f"Directional solidification {n}^3 (benchmark workload)",
+        "*****",
+        "Problem type: C",
+        "Decomposition strategy: 1",
+        "Material: Inconel625",
+        "Cell size (microns): 1",
+        "Heterogeneous nucleation density (normalized by 1*10^12 per m^3): 100",
+        "Mean nucleation undercooling (in K): 3",
+        "Standard deviation of nucleation undercooling: 0.5",
+        "Path to output: ./",
+        "Output file base name: bench",
+        "File of grain orientations: GrainOrientationVectors_Uniform10k.csv",
+        "Thermal gradient (K/m): 1000000",
+        "Cooling rate (K/s): 1000000",
+        f"Domain size in x: {n}",
+        f"Domain size in y: {n}",
+        f"Domain size in z: {n}",
+        '"N", where the time step = deltax/(Steady State Velocity * N): 25',
+        "Fraction of surface sites active: 0.02",
+        "***Output data printing options: (Y or N) which data should be printed***",
+        "Print Paraview vtk file of grain misorientation values (Y or N)?: N",
+        "Print Paraview vtk file of all ExaCA data for post-processing (Y or N)?: N",
+        "Debug check (reduced)- Print data for main Kokkos views (CellType, LayerID, CritTimeStep) following initialization for debug check (Y or N)?: N",
+        "Debug check (extensive) - Print data for all main data structures (CellType, GrainID, CritTimeStep, UndercoolingCurrent, UndercoolingChange, Melted, LayerID) following initialization for debug check (Y or N)?: N",
+    ]) + "\n"
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except FileNotFoundError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def run_reference_sample(n, samples, cycles_per_sample, threads):
+    """The reference's own CPU path (OpenMP build) on bounded samples of the workload."""
+    if not os.path.exists(REF_BENCH):
+        raise FileNotFoundError(REF_BENCH)
+    with tempfile.TemporaryDirectory() as d:
+        inp = os.path.join(d, "bench.txt")
+        with open(inp, "w") as f:
+            f.write(input_file_text(n))
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close",
+                   EXACA_DATA_DIR=os.path.join(ROOT, "exaca_b200", "data"))
+        r = subprocess.run([REF_BENCH, inp, str(samples), str(cycles_per_sample)], cwd=d, env=env,
+                           capture_output=True, text=True, check=True)
+        line = [ln for ln in r.stdout.splitlines() if "{\"cycles\"" in ln][-1]
+        return json.loads(line[line.index("{"):])
+
+
+def reference_arm(args, rank, world):
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    res = run_reference_sample(args.size, args.warmup + args.steps, args.ref_cycles, threads)
+    timed = res["sample_s"][args.warmup:]
+    cells = res["active_domain_cells"]
+    cycles = res["cycles_per_sample"] * len(timed)
+    value = cells * cycles / sum(timed)
+    n = args.size
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32 (reference mixed precision)", "data": "synthetic",
+        "config": {"workload": f"directional solidification {n}^3, G=R=1e6, N=25, 1e14 m^-3 nuclei",
+                   "cells": cells, "step": f"{args.ref_cycles} CA cycles of the reference's OpenMP CPU path",
+                   "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                         "sample": f"CA cycles {args.warmup * args.ref_cycles + 1}-{res['cycles']} of the {n}^3 "
+                                   f"solve after the reference's own initialisation ({res['init_s']:.1f} s)"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def b200_arm(args, rank, world, local):
+    import numpy as np
+    import torch
+
+    import exaca_b200 as ex
+
+    if not os.path.exists(ex.LIB_PATH):
+        from exaca_b200 import build as b
+
+        b.build()
+    device = local
+    torch.cuda.set_device(device)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=torch.device("cuda", device))
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    n = args.size
+    t0 = time.perf_counter()
+    prob = ex.Problem.directional(n, n, n, **WORKLOAD)
+    prob.pin()
+    init_s = time.perf_counter() - t0
+    g = prob.geometry
+    cells = g.active_size
+    pool = ex.Pool(device, list_capacity=cells)
+
+    def solve():
+        slot = pool.admit(prob, device_check=False)
+        cyc = pool.run_plain(slot)
+        ms = pool.last_run_ms()
+        pool.retire(slot)
+        return cyc, ms
+
+    for _ in range(args.warmup):
+        solve()
+    barrier()
+    st0 = pool.stats()
+    clocks = ClockSampler(device)
+    clocks.start()
+    times, cycles = [], []
+    for _ in range(args.steps):
+        c, ms = solve()
+        times.append(ms)
+        cycles.append(c)
+    clock_info = clocks.stop()
+    barrier()
+    st1 = pool.stats()
+    total_ms = max_over_ranks(sum(times))
+    cell_updates = cells * sum(cycles)
+    value = world * cell_updates / (total_ms / 1e3)
+    launches = st1["launches"] - st0["launches"] + sum(c // 1000 + 1 for c in cycles)  # + one census per 1000 cycles
+
+    # end to end through the C ABI from pinned host buffers: upload, solve, download GrainID/CellType
+    gid = torch.empty(g.domain_size, dtype=torch.int32, pin_memory=True)
+    ct = torch.empty(g.domain_size, dtype=torch.int32, pin_memory=True)
+    lib = ex.load_library()
+    barrier()
+    t_e = time.perf_counter()
+    slot = pool.admit(prob, device_check=False)
+    c_e = pool.run_plain(slot)
+    rc = lib.exaca_pool_copy_out(pool._h, slot, gid.data_ptr(), ct.data_ptr())
+    e2e_s = time.perf_counter() - t_e
+    if rc != 0:
+        raise RuntimeError(lib.exaca_last_error())
+    pool.retire(slot)
+    e2e_s = max_over_ranks(e2e_s)
+    h2d = g.domain_size * (1 + 4 + 4 + 1 + 4) + 8 * g.n_nuclei
+    d2h = 8 * g.domain_size
+    e2e_value = world * cells * c_e / e2e_s
+
+    # roofline of the dominant step kernel on a bounded stretch of the solve, CUDA events per launch
+    slot = pool.admit(prob, device_check=False)
+    pool.step(args.profile_at)
+    pa = pool.stats()
+    kt = pool.profile_cycles(args.profile_cycles)
+    pb = pool.stats()
+    pool.retire(slot)
+    d = {k: pb[k] - pa[k] for k in pb}
+    grow_bytes = sum(GROW_BYTES[k] * d[k] for k in GROW_BYTES)
+    cap_bytes = sum(CAPTURE_BYTES[k] * d[k] for k in CAPTURE_BYTES)
+    kernels = {"k_grow_claim": (kt["grow_ms"], grow_bytes), "k_capture": (kt["capture_ms"], cap_bytes)}
+    dom = max(kernels, key=lambda k: kernels[k][0])
+    dom_ms, dom_bytes = kernels[dom]
+    peak, peak_kind = peaks()
+    achieved = dom_bytes / (dom_ms / 1e3) / 1e9
+    per_launch_bytes = dom_bytes / max(1, args.profile_cycles)
+    traffic = None
+    traffic_file = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
+    if os.path.exists(traffic_file):
+        for ln in open(traffic_file):
+            if ln.startswith(dom + " "):
+                traffic = float(ln.split()[1])
+
+    # dense-equivalent effective roofline (the reference formulation's compulsory bytes per cycle)
+    eff_bytes_per_update = 14.5
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32 (reference mixed precision), int32/int8",
+            "data": "synthetic (generated by the solver's own seeded initialisation)",
+            "config": {"workload": f"directional solidification {n}^3, G=R=1e6 K/m|K/s, N=25, 1e14 m^-3 nuclei",
+                       "cells": cells, "cycles": cycles, "step": "one full solve to termination",
+                       "l2": "state (~148 B/cell, > L2) re-uploaded between steps", "replicas": world,
+                       "host_init_s": round(init_s, 2)},
+            "clocks": clock_info,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "seconds": e2e_s},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": per_launch_bytes,
+                         "sample": f"cycles {args.profile_at + 1}-{args.profile_at + args.profile_cycles}",
+                         "kernel_ms": {k: v[0] / max(1, args.profile_cycles) for k, v in kernels.items()},
+                         "effective_dense_frac": value / world * eff_bytes_per_update / 1e9 / peak},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            try:
+                threads = os.cpu_count() or 1
+                res = run_reference_sample(n, 1, args.ref_cycles, threads)
+                v = res["active_domain_cells"] * res["cycles_per_sample"] / res["sample_s"][0]
+                line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                                        "sample": f"CA cycles 1-{res['cycles']} of the same {n}^3 solve, reference "
+                                                  f"OpenMP CPU path after its own initialisation"}
+            except Exception as e:  # the baseline is reported, never required
+                line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
+                                        "sample": f"unavailable: {e}"}
+        print(json.dumps(line), flush=True)
+    pool.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--size", type=int, default=512)
+    ap.add_argument("--ref-cycles", type=int, default=40, help="CA cycles per reference sample")
+    ap.add_argument("--profile-at", type=int, default=6000)
+    ap.add_argument("--profile-cycles", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+    else:
+        b200_arm(args, rank, world, local)
+
+
+if __name__ == "__main__":
+    main()

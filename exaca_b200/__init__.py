@@ -67,9 +67,13 @@ class DirsParams(ctypes.Structure):
 class DomainStatus(ctypes.Structure):
     _fields_ = [
         ("cycle", ctypes.c_int), ("done", ctypes.c_int), ("nn", ctypes.c_int), ("error", ctypes.c_int),
-        ("liquid", ctypes.c_int64), ("n_grown", ctypes.c_uint64), ("n_captured", ctypes.c_uint64),
-        ("n_listed", ctypes.c_uint64),
+        ("liquid", ctypes.c_int64),
     ]
+
+
+class PoolStatsT(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_uint64) for n in
+                ("cycles", "launches", "listed", "grown", "captured", "nucleated", "claims", "liquid_nb", "kept")]
 
 
 class CensusT(ctypes.Structure):
@@ -94,12 +98,16 @@ SIGNATURES = {
     "exaca_pool_step": ([_P, _I], _I),
     "exaca_pool_status": ([_P, _I, ctypes.POINTER(DomainStatus)], _I),
     "exaca_pool_census": ([_P, _I, ctypes.POINTER(CensusT)], _I),
+    "exaca_pool_stats": ([_P, ctypes.POINTER(PoolStatsT)], _I),
     "exaca_pool_run_plain": ([_P, _I, _I, ctypes.POINTER(_I)], _I),
     "exaca_pool_copy_out": ([_P, _I, _P, _P], _I),
     "exaca_pool_copy_octahedra": ([_P, _I, _P, _P, _P], _I),
     "exaca_pool_retire": ([_P, _I], _I),
     "exaca_pool_bytes_in_use": ([_P], ctypes.c_int64),
     "exaca_pool_write_outputs": ([_P, _I, _P, ctypes.c_char_p], _I),
+    "exaca_pool_last_run_ms": ([_P], ctypes.c_double),
+    "exaca_pool_profile_cycles": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
+    "exaca_problem_pin": ([_P], _I),
 }
 
 _lib = None
@@ -181,6 +189,10 @@ class Problem:
     def slot_bytes(self) -> int:
         return int(load_library().exaca_problem_slot_bytes(self._h))
 
+    def pin(self) -> None:
+        """Page-locks the host fields so admission copies run at full PCIe bandwidth."""
+        _check(load_library().exaca_problem_pin(self._h))
+
     def __del__(self):
         if getattr(self, "_h", None) and _lib is not None:
             _lib.exaca_problem_free(self._h)
@@ -194,9 +206,6 @@ class Status:
     nn: int
     error: int
     liquid: int
-    n_grown: int
-    n_captured: int
-    n_listed: int
 
 
 class Pool:
@@ -219,7 +228,12 @@ class Pool:
     def status(self, slot: int) -> Status:
         s = DomainStatus()
         _check(load_library().exaca_pool_status(self._h, slot, ctypes.byref(s)))
-        return Status(s.cycle, bool(s.done), s.nn, s.error, s.liquid, s.n_grown, s.n_captured, s.n_listed)
+        return Status(s.cycle, bool(s.done), s.nn, s.error, s.liquid)
+
+    def stats(self) -> dict:
+        s = PoolStatsT()
+        _check(load_library().exaca_pool_stats(self._h, ctypes.byref(s)))
+        return {n: getattr(s, n) for n, _ in PoolStatsT._fields_}
 
     def census(self, slot: int) -> dict:
         c = CensusT()
@@ -245,6 +259,16 @@ class Pool:
         cdl = np.empty(26 * a, np.float32)
         _check(load_library().exaca_pool_copy_octahedra(self._h, slot, _ptr(dl), _ptr(doc), _ptr(cdl)))
         return dl, doc, cdl
+
+    def last_run_ms(self) -> float:
+        """CUDA-event device time of the last run_plain on this pool."""
+        return float(load_library().exaca_pool_last_run_ms(self._h))
+
+    def profile_cycles(self, n_cycles: int) -> dict:
+        """Runs n cycles kernel by kernel with CUDA events around each launch; summed ms per kernel."""
+        t = (ctypes.c_double * 3)()
+        _check(load_library().exaca_pool_profile_cycles(self._h, n_cycles, t))
+        return {"begin_ms": t[0], "grow_ms": t[1], "capture_ms": t[2]}
 
     def retire(self, slot: int) -> None:
         _check(load_library().exaca_pool_retire(self._h, slot))

@@ -144,7 +144,11 @@ int exaca_problem_directional(const exaca_dirs_params *prm, exaca_problem **out)
     });
 }
 
-void exaca_problem_free(exaca_problem *p) { delete p; }
+void exaca_problem_free(exaca_problem *p) {
+    if (p && p->p && p->p.use_count() == 1)
+        exaca::unpin_problem(*p->p);
+    delete p;
+}
 
 int exaca_problem_info(const exaca_problem *p, exaca_problem_geometry *info) {
     if (!p || !info)
@@ -217,11 +221,44 @@ int exaca_pool_status(exaca_pool *pool, int slot, exaca_domain_status *st) {
         st->done = d.done;
         st->nn = d.nn;
         st->error = d.error | pool->pool->pool_error();
-        st->liquid = d.liquid;
-        st->n_grown = d.n_grown;
-        st->n_captured = d.n_captured;
-        st->n_listed = d.n_listed;
+        st->liquid = pool->pool->liquid(slot);
     });
+}
+
+int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st) {
+    if (!pool || !st)
+        return fail(EXACA_ERR_ARG, "null argument");
+    return guarded([&] {
+        exaca::PoolStats s = pool->pool->stats();
+        st->cycles = s.cycles;
+        st->launches = s.launches;
+        st->listed = s.listed;
+        st->grown = s.grown;
+        st->captured = s.captured;
+        st->nucleated = s.nucleated;
+        st->claims = s.claims;
+        st->liquid_nb = s.liquid_nb;
+        st->kept = s.kept;
+    });
+}
+
+double exaca_pool_last_run_ms(exaca_pool *pool) { return pool ? pool->pool->last_run_ms() : -1.0; }
+
+int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms) {
+    if (!pool || !kernel_ms || n_cycles < 0)
+        return fail(EXACA_ERR_ARG, "bad argument");
+    return guarded([&] {
+        exaca::KernelTimes t = pool->pool->profile_cycles(n_cycles);
+        kernel_ms[0] = t.begin_ms;
+        kernel_ms[1] = t.grow_ms;
+        kernel_ms[2] = t.capture_ms;
+    });
+}
+
+int exaca_problem_pin(exaca_problem *p) {
+    if (!p)
+        return fail(EXACA_ERR_ARG, "null argument");
+    return guarded([&] { exaca::pin_problem(*p->p); });
 }
 
 int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c) {

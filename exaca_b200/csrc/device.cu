@@ -42,15 +42,18 @@ namespace exaca {
 __constant__ int c_nx[26];
 __constant__ int c_ny[26];
 __constant__ int c_nz[26];
-__constant__ int c_itlist[9][26];
-__constant__ int c_itlen[9];
+// ItList (src/CAinitialize.cpp:676-745) as 26-bit direction masks per edge case, and the directions
+// with a z component of +1 / -1
+__constant__ unsigned int c_itmask[9];
+__constant__ unsigned int c_zplus;
+__constant__ unsigned int c_zminus;
 
 constexpr unsigned int kMaskCarry = 1u << 30; // not eligible this cycle: keep in the list
 constexpr unsigned int kMaskDrop = 1u << 31;  // domain finished: leave the list
 constexpr int kErrGrowthTable = 1;
 constexpr int kErrListOverflow = 2;
 constexpr int kErrBounds = 4;
-constexpr int kErrJumps = 8;
+constexpr int kBlock = 256;
 
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; } // std::min
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; } // std::max
@@ -69,79 +72,135 @@ __device__ __forceinline__ long long executed_upto(const DomainDesc &D, long lon
     return e;
 }
 
-// Warp-aggregated append of `n` entries per lane; returns this lane's base (or ULLONG_MAX on overflow).
-__device__ __forceinline__ unsigned long long warp_reserve(PoolState *P, int slot, unsigned int n) {
-    unsigned int lane = threadIdx.x & 31;
+// Block-aggregated reservation of `n` list slots per thread: one atomicAdd per block. Must be
+// called by every thread of the block. Returns this thread's first slot, or ULLONG_MAX on overflow.
+__device__ __forceinline__ unsigned long long block_reserve(PoolState *P, int slot, unsigned int n) {
+    __shared__ unsigned int s_warp[kBlock / 32];
+    __shared__ unsigned long long s_base;
+    __shared__ int s_ok;
+    const unsigned int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     unsigned int incl = n;
+#pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
         if (lane >= (unsigned)o)
             incl += v;
     }
-    unsigned int total = __shfl_sync(0xffffffffu, incl, 31);
-    unsigned long long base = 0;
-    if (lane == 31 && total)
-        base = atomicAdd(&P->cnt[slot], (unsigned long long)total);
-    base = __shfl_sync(0xffffffffu, base, 31);
-    if (base + total > P->capacity) {
-        if (lane == 0 && total)
-            atomicOr(&P->error, kErrListOverflow);
-        return ULLONG_MAX;
+    if (lane == 31)
+        s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        unsigned int v = lane < kBlock / 32 ? s_warp[lane] : 0;
+        unsigned int inc2 = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned int u = __shfl_up_sync(0xffffffffu, inc2, o);
+            if (lane >= (unsigned)o)
+                inc2 += u;
+        }
+        if (lane < kBlock / 32)
+            s_warp[lane] = inc2 - v;
+        unsigned int total = __shfl_sync(0xffffffffu, inc2, kBlock / 32 - 1);
+        if (lane == 0) {
+            unsigned long long b = total ? atomicAdd(&P->cnt[slot], (unsigned long long)total) : 0ull;
+            s_ok = (b + total <= P->capacity);
+            if (!s_ok)
+                atomicOr(&P->error, kErrListOverflow);
+            s_base = b;
+        }
     }
-    return base + (incl - n);
+    __syncthreads();
+    unsigned long long r = s_ok ? s_base + s_warp[warp] + (incl - n) : ULLONG_MAX;
+    __syncthreads(); // s_warp / s_base are reused by the next call
+    return r;
 }
 
-// Warp-aggregated per-domain counter update (lanes grouped by domain id).
-__device__ __forceinline__ void warp_add_domain(DomainDesc *desc, unsigned int dom, long long v,
-                                                unsigned long long DomainDesc::*field) {
-    unsigned int peers = __match_any_sync(0xffffffffu, dom);
-    int leader = __ffs(peers) - 1;
-    long long sum = 0;
-    for (unsigned int m = peers; m; m &= m - 1) {
-        int src = __ffs(m) - 1;
-        sum += __shfl_sync(peers, v, src);
+// Block-level sum of per-thread statistics into one shard of the pool counters.
+__device__ __forceinline__ void block_stats(PoolState *P, unsigned long long a, unsigned long long b, int ia, int ib) {
+    __shared__ unsigned long long s_a[kBlock / 32], s_b[kBlock / 32];
+    for (int o = 16; o; o >>= 1) {
+        a += __shfl_down_sync(0xffffffffu, a, o);
+        b += __shfl_down_sync(0xffffffffu, b, o);
     }
-    if ((int)(threadIdx.x & 31) == leader && sum)
-        atomicAdd(&(desc[dom].*field), (unsigned long long)sum);
+    if ((threadIdx.x & 31) == 0) {
+        s_a[threadIdx.x >> 5] = a;
+        s_b[threadIdx.x >> 5] = b;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long ta = 0, tb = 0;
+        for (int w = 0; w < kBlock / 32; w++) {
+            ta += s_a[w];
+            tb += s_b[w];
+        }
+        int shard = blockIdx.x & (kStatShards - 1);
+        if (ta)
+            atomicAdd(&P->stat[shard][ia], ta);
+        if (tb)
+            atomicAdd(&P->stat[shard][ib], tb);
+    }
 }
 
-__device__ __forceinline__ void warp_add_liquid(DomainDesc *desc, unsigned int dom, long long v) {
-    unsigned int peers = __match_any_sync(0xffffffffu, dom);
-    int leader = __ffs(peers) - 1;
-    long long sum = 0;
-    for (unsigned int m = peers; m; m &= m - 1) {
-        int src = __ffs(m) - 1;
-        sum += __shfl_sync(peers, v, src);
-    }
-    if ((int)(threadIdx.x & 31) == leader && sum)
-        atomicAdd((unsigned long long *)&desc[dom].liquid, (unsigned long long)(-sum));
+__device__ __forceinline__ void cell_coords(const DomainDesc &D, unsigned int c, int &rx, int &ry, int &rz) {
+    unsigned int plane = (unsigned int)(D.mx * D.my);
+    unsigned int z = c / plane;
+    unsigned int rem = c - z * plane;
+    unsigned int x = rem / (unsigned int)D.my;
+    rz = (int)z;
+    rx = (int)x;
+    ry = (int)(rem - x * (unsigned int)D.my);
+}
+
+// Edge case of src/CAfunctions.cpp:169-213 as a direction mask, restricted to the active window in z.
+__device__ __forceinline__ unsigned int neighbour_mask(const DomainDesc &D, int rx, int ry, int rz) {
+    int b = (ry == 0) ? (rx == 0 ? 5 : (rx == D.mx - 1 ? 6 : 1))
+                      : (ry == D.my - 1 ? (rx == 0 ? 7 : (rx == D.mx - 1 ? 8 : 2))
+                                        : (rx == 0 ? 3 : (rx == D.mx - 1 ? 4 : 0)));
+    unsigned int m = c_itmask[b];
+    if (rz + 1 >= D.nz_active)
+        m &= ~c_zplus;
+    if (rz - 1 < 0)
+        m &= ~c_zminus;
+    return m;
+}
+
+__device__ __forceinline__ long long nb_offset(int l, int plane, int my) {
+    return (long long)c_nz[l] * plane + c_nx[l] * my + c_ny[l];
 }
 
 // Fresh octahedron of a newly active cell at its own centre (src/CAupdate.cpp:100-194,
 // src/CAinitialize.cpp:1942-2042): DL = 0.01, centre = cell centre, CDL from the orientation table.
-__device__ void make_fresh_octahedron(const DomainDesc &D, long long c) {
-    int plane = D.mx * D.my;
-    int rz = (int)(c / plane);
-    int rem = (int)(c - (long long)rz * plane);
-    int rx = rem / D.my, ry = rem - (rem / D.my) * D.my;
+__device__ void make_fresh_octahedron(const DomainDesc &D, unsigned int c) {
+    int rx, ry, rz;
+    cell_coords(D, c, rx, ry, rz);
     int h = D.gid[c];
     int ori = (abs(h) - 1) % 10000;
     if (ori < 0)
         ori += 10000;
     D.dl[c] = 0.01f;
-    D.doc[3 * c + 0] = (float)((double)(rx + D.xoff) + 0.5);
-    D.doc[3 * c + 1] = (float)((double)(ry + D.yoff) + 0.5);
-    D.doc[3 * c + 2] = (float)((double)rz + 0.5);
-    const float *t = D.cdl_table + 26 * ori;
-    float *o = D.cdl + 26 * c;
+    D.doc[3ull * c + 0] = (float)((double)(rx + D.xoff) + 0.5);
+    D.doc[3ull * c + 1] = (float)((double)(ry + D.yoff) + 0.5);
+    D.doc[3ull * c + 2] = (float)((double)rz + 0.5);
+    const float2 *t = reinterpret_cast<const float2 *>(D.cdl_table + 26 * ori);
+    float2 *o = reinterpret_cast<float2 *>(D.cdl + 26ull * c);
 #pragma unroll
-    for (int n = 0; n < 26; n++)
+    for (int n = 0; n < 13; n++)
         o[n] = t[n];
 }
 
+__device__ __forceinline__ long long domain_liquid(const DomainDesc &D) {
+    long long v = D.liquid;
+#pragma unroll
+    for (int q = 0; q < kLiquidShards; q++)
+        v += __ldcg(&D.liquid_shard[q]);
+    return v;
+}
+
 // ---------------------------------------------------------------------------------------------
-// k_step_begin: one block; warp w serves domains w, w + nwarps, ...
-__global__ void k_step_begin(PoolState *P) {
+// Start of a CA cycle for every domain (src/runCA.cpp:290-298, src/CAupdate.cpp:67-200), run by one
+// block: list swap, device-side termination check, cycle advance, nucleation. Reads that may see
+// data other blocks of the same kernel wrote go through L2 (__ldcg).
+__device__ void begin_cycle(PoolState *P) {
     __shared__ int s_cur;
     if (threadIdx.x == 0) {
         // the list built by the previous cycle becomes current; the consumed one is reset
@@ -151,19 +210,20 @@ __global__ void k_step_begin(PoolState *P) {
         s_cur = cur;
     }
     __syncthreads();
-    int cur = s_cur;
-    int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    const int cur = s_cur;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    unsigned long long nucleated = 0;
     for (int d = warp; d < P->n_domains; d += nwarps) {
         DomainDesc &D = P->desc[d];
         if (D.ctype == nullptr || D.done)
             continue;
-        if (D.check_mode && D.cycle > 0 && D.cycle % 1000 == 0 && D.liquid == 0) {
+        if (D.check_mode && D.cycle > 0 && D.cycle % 1000 == 0 && domain_liquid(D) == 0) {
             // src/CAupdate.cpp:782-783: no superheated or undercooled liquid left
             if (lane == 0)
                 D.done = 1;
             continue;
         }
-        int cycle = D.cycle + 1;
+        const int cycle = D.cycle + 1;
         __syncwarp();
         if (lane == 0) {
             D.cycle = cycle;
@@ -179,15 +239,15 @@ __global__ void k_step_begin(PoolState *P) {
             // nuclei are sorted by time, so the due ones form a prefix
             int n_due = __popc(due);
             bool fire = false;
-            long long loc = 0;
+            unsigned int loc = 0;
             if (t <= cycle) {
-                loc = D.nuc_loc[idx];
-                if (loc < 0 || loc >= D.active_size) {
+                int l = D.nuc_loc[idx];
+                if (l < 0 || l >= D.active_size) {
                     atomicOr(&D.error, kErrBounds);
-                    loc = 0;
                 }
                 else {
-                    fire = D.ctype[loc] == kLiquid && D.layer[loc] <= 0;
+                    loc = (unsigned int)l;
+                    fire = __ldcg(D.ctype + loc) == kLiquid && D.layer[loc] <= 0;
                 }
                 if (fire)
                     make_fresh_octahedron(D, loc);
@@ -199,13 +259,10 @@ __global__ void k_step_begin(PoolState *P) {
                 if (rank == 0)
                     base = atomicAdd(&P->cnt[cur], (unsigned long long)__popc(fired));
                 base = __shfl_sync(fired, base, __ffs(fired) - 1);
-                if (base + __popc(fired) > P->capacity) {
+                if (base + __popc(fired) > P->capacity)
                     atomicOr(&P->error, kErrListOverflow);
-                }
-                else {
+                else
                     P->list[cur][base + rank] = ((unsigned long long)d << 32) | (unsigned long long)loc;
-                }
-                __threadfence();
                 D.ctype[loc] = kActive;
             }
             fired_total += __popc(fired);
@@ -217,83 +274,99 @@ __global__ void k_step_begin(PoolState *P) {
             D.nuc_cursor = cursor;
             D.nn += fired_total;
             D.liquid -= fired_total;
+            nucleated += fired_total;
         }
     }
+    if (lane == 0 && nucleated)
+        atomicAdd(&P->stat[0][kStatNucleated], nucleated);
 }
+
+__global__ void k_step_begin(PoolState *P) { begin_cycle(P); }
 
 // ---------------------------------------------------------------------------------------------
 // k_grow_claim: src/CAupdate.cpp:217-352 for every listed active cell
-__global__ void __launch_bounds__(256) k_grow_claim(PoolState *P) {
+__global__ void __launch_bounds__(kBlock) k_grow_claim(PoolState *P) {
     const int cur = P->cur;
     const unsigned long long n = P->cnt[cur];
     const unsigned long long *list = P->list[cur];
     unsigned int *mask = P->mask;
     DomainDesc *desc = P->desc;
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long i0 = (unsigned long long)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
-        unsigned long long i = i0 + threadIdx.x;
-        bool valid = i < n;
-        unsigned int dom = 0;
-        long long grown = 0;
-        if (valid) {
-            unsigned long long e = list[i];
-            dom = (unsigned int)(e >> 32);
-            long long c = (long long)(e & 0xffffffffull);
-            DomainDesc &D = desc[dom];
-            unsigned int m;
-            if (D.done) {
-                m = kMaskDrop;
+    const unsigned long long stride = (unsigned long long)gridDim.x * kBlock;
+    unsigned long long st_listed = 0, st_grown = 0, st_claims = 0, st_liq = 0;
+    for (unsigned long long i = (unsigned long long)blockIdx.x * kBlock + threadIdx.x; i < n; i += stride) {
+        unsigned long long e = list[i];
+        unsigned int dom = (unsigned int)(e >> 32);
+        unsigned int c = (unsigned int)e;
+        DomainDesc &D = desc[dom];
+        st_listed++;
+        unsigned int m;
+        if (D.done) {
+            m = kMaskDrop;
+        }
+        else {
+            const int cycle = D.cycle;
+            const int cts = D.cts[c];
+            // single-layer problems only (checked at admission): LayerID <= layer always holds
+            if (!(cycle > cts)) {
+                m = kMaskCarry;
             }
             else {
-                int cycle = D.cycle;
-                int cts = D.cts[c];
-                if (!(cycle > cts) || D.layer[c] > 0) {
-                    m = kMaskCarry;
+                st_grown++;
+                // undercooling after the executed updates since the liquidus (src/CAupdate.cpp:236-237)
+                long long nu = executed_upto(D, cycle) - executed_upto(D, cts);
+                if (D.zero_du && D.du[c] == 0.0f)
+                    nu = 0;
+                double inc = 0.0;
+                if (nu >= 0 && nu < D.growth_len)
+                    inc = __ldg(D.growth + nu);
+                else
+                    atomicOr(&D.error, kErrGrowthTable);
+                const float dl = (float)((double)D.dl[c] + inc);
+                D.dl[c] = dl;
+                int rx, ry, rz;
+                cell_coords(D, c, rx, ry, rz);
+                const unsigned int valid = neighbour_mask(D, rx, ry, rz);
+                const int plane = D.mx * D.my, my = D.my;
+                const int8_t *ct = D.ctype + c;
+                // the 26 critical lengths as 13 aligned 8-byte loads (26 * 4 * c is 8-byte aligned),
+                // issued together with the 26 independent neighbour-type loads
+                const float2 *row = reinterpret_cast<const float2 *>(D.cdl + 26ull * c);
+                float cdl[26];
+#pragma unroll
+                for (int q = 0; q < 13; q++) {
+                    float2 v = row[q];
+                    cdl[2 * q] = v.x;
+                    cdl[2 * q + 1] = v.y;
                 }
-                else {
-                    grown = 1;
-                    long long nu = 0;
-                    if (D.du[c] != 0.0f)
-                        nu = executed_upto(D, cycle) - executed_upto(D, cts);
-                    double inc = 0.0;
-                    if (nu >= 0 && nu < D.growth_len)
-                        inc = __ldg(D.growth + nu);
-                    else
-                        atomicOr(&D.error, kErrGrowthTable);
-                    float dl = (float)((double)D.dl[c] + inc);
-                    D.dl[c] = dl;
-                    int plane = D.mx * D.my;
-                    int rz = (int)(c / plane);
-                    int rem = (int)(c - (long long)rz * plane);
-                    int rx = rem / D.my;
-                    int ry = rem - rx * D.my;
-                    int b = (ry == 0) ? (rx == 0 ? 5 : (rx == D.mx - 1 ? 6 : 1))
-                                      : (ry == D.my - 1 ? (rx == 0 ? 7 : (rx == D.mx - 1 ? 8 : 2))
-                                                        : (rx == 0 ? 3 : (rx == D.mx - 1 ? 4 : 0)));
-                    unsigned long long key =
-                        ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
-                    const float *cdl = D.cdl + 26 * c;
-                    unsigned int liq = 0;
-                    int len = c_itlen[b];
-                    for (int ll = 0; ll < len; ll++) {
-                        int l = c_itlist[b][ll];
-                        int nzz = rz + c_nz[l];
-                        if (nzz >= D.nz_active || nzz < 0)
-                            continue;
-                        long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
-                        if (D.ctype[t] == kLiquid) {
+                unsigned int liq = 0;
+#pragma unroll
+                for (int l = 0; l < 26; l++) {
+                    if (valid & (1u << l)) {
+                        if (ct[nb_offset(l, plane, my)] == kLiquid)
                             liq |= 1u << l;
-                            if (dl >= cdl[l])
-                                atomicMin(&D.claim[t], key);
+                    }
+                }
+                if (liq) {
+                    const unsigned long long key =
+                        ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
+                    unsigned long long *claim = D.claim + c;
+#pragma unroll
+                    for (int l = 0; l < 26; l++) {
+                        if ((liq & (1u << l)) && dl >= cdl[l]) {
+                            atomicMin(claim + nb_offset(l, plane, my), key);
+                            st_claims++;
                         }
                     }
-                    m = liq;
                 }
+                st_liq += __popc(liq);
+                m = liq;
             }
-            mask[i] = m;
         }
-        warp_add_domain(desc, valid ? dom : 0xffffffffu, grown, &DomainDesc::n_grown);
+        mask[i] = m;
     }
+    block_stats(P, st_listed, st_grown, kStatListed, kStatGrown);
+    __syncthreads();
+    block_stats(P, st_claims, st_liq, kStatClaims, kStatLiquidNb);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -419,7 +492,16 @@ __device__ void capture_cell(const DomainDesc &D, long long c, long long t, int 
 }
 
 // k_capture: captures won, solidification (src/CAupdate.cpp:336-352, 722-725), next list.
-__global__ void __launch_bounds__(256) k_capture(PoolState *P) {
+// The capture geometry (a long double-precision dependency chain) is spread over the block: every
+// won (capturer, target, direction) triple goes to shared memory and the block's threads take one
+// each. With kTail the last block to finish also starts the next cycle (begin_cycle).
+constexpr int kCaptureSlots = 1024;
+
+template <bool kTail> __global__ void __launch_bounds__(kBlock) k_capture(PoolState *P) {
+    __shared__ unsigned int s_c[kCaptureSlots], s_t[kCaptureSlots];
+    __shared__ unsigned short s_dom[kCaptureSlots];
+    __shared__ unsigned char s_l[kCaptureSlots];
+    __shared__ unsigned int s_ncap;
     const int cur = P->cur;
     const int nxt = cur ^ 1;
     const unsigned long long n = P->cnt[cur];
@@ -427,88 +509,123 @@ __global__ void __launch_bounds__(256) k_capture(PoolState *P) {
     unsigned long long *out = P->list[nxt];
     const unsigned int *mask = P->mask;
     DomainDesc *desc = P->desc;
-    const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
-    for (unsigned long long i0 = (unsigned long long)blockIdx.x * blockDim.x; i0 < n; i0 += stride) {
-        unsigned long long i = i0 + threadIdx.x;
-        bool valid = i < n;
-        unsigned int dom = 0xffffffffu;
+    const unsigned long long stride = (unsigned long long)gridDim.x * kBlock;
+    unsigned long long st_captured = 0, st_kept = 0;
+    // block-uniform loop so that block_reserve is reached by every thread
+    for (unsigned long long i0 = (unsigned long long)blockIdx.x * kBlock; i0 < n; i0 += stride) {
+        const unsigned long long i = i0 + threadIdx.x;
+        const bool valid = i < n;
         unsigned long long e = 0;
         unsigned int m = kMaskDrop;
         if (valid) {
             e = list[i];
-            dom = (unsigned int)(e >> 32);
             m = mask[i];
         }
-        // captured targets of this lane, as neighbour directions
+        const unsigned int dom = (unsigned int)(e >> 32);
+        const unsigned int c = (unsigned int)e;
         unsigned int won = 0;
         bool keep = false;
-        long long c = (long long)(e & 0xffffffffull);
-        if (valid && !(m & kMaskDrop)) {
+        int plane = 0, my = 0;
+        if (!(m & kMaskDrop)) {
             if (m & kMaskCarry) {
                 keep = true;
             }
             else {
                 const DomainDesc &D = desc[dom];
-                int plane = D.mx * D.my;
-                unsigned int want = 0xffffffffu - D.epoch;
+                plane = D.mx * D.my;
+                my = D.my;
+                const unsigned int want = 0xffffffffu - D.epoch;
+                const unsigned long long *claim = D.claim + c;
                 bool lcount = false;
-                for (unsigned int bits = m; bits; bits &= bits - 1) {
-                    int l = __ffs(bits) - 1;
-                    long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
-                    unsigned long long k = D.claim[t];
-                    if ((unsigned int)(k >> 32) == want) {
-                        long long w = (long long)(k & 0xffffffffull);
-                        if (w >= c)
+#pragma unroll
+                for (int l = 0; l < 26; l++) {
+                    if (m & (1u << l)) {
+                        unsigned long long k = claim[nb_offset(l, plane, my)];
+                        if ((unsigned int)(k >> 32) == want) {
+                            unsigned int w = (unsigned int)k;
+                            if (w >= c)
+                                lcount = true;
+                            if (w == c)
+                                won |= 1u << l;
+                        }
+                        else {
                             lcount = true;
-                        if (w == c)
-                            won |= 1u << l;
+                        }
                     }
-                    else {
-                        lcount = true;
-                    }
-                }
-                for (unsigned int bits = won; bits; bits &= bits - 1) {
-                    int l = __ffs(bits) - 1;
-                    long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
-                    capture_cell(D, c, t, l);
                 }
                 if (!lcount)
                     D.ctype[c] = kSolid;
                 keep = lcount;
             }
         }
-        unsigned int n_out = (keep ? 1u : 0u) + (unsigned int)__popc(won);
-        unsigned long long base = warp_reserve(P, nxt, n_out);
-        if (base != ULLONG_MAX && n_out) {
-            unsigned long long hi = (unsigned long long)dom << 32;
+        const unsigned int ncap = (unsigned int)__popc(won);
+        const unsigned int n_out = (keep ? 1u : 0u) + ncap;
+        if (threadIdx.x == 0)
+            s_ncap = 0;
+        const unsigned long long base = block_reserve(P, nxt, n_out);
+        unsigned int spill = 0; // triples that do not fit in shared memory stay with this thread
+        if (n_out) {
             unsigned long long pos = base;
-            if (keep)
+            if (keep && base != ULLONG_MAX)
                 out[pos++] = e;
-            if (won) {
-                const DomainDesc &D = desc[dom];
-                int plane = D.mx * D.my;
-                for (unsigned int bits = won; bits; bits &= bits - 1) {
-                    int l = __ffs(bits) - 1;
-                    long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
+            const unsigned long long hi = (unsigned long long)dom << 32;
+            unsigned int slot0 = ncap ? atomicAdd(&s_ncap, ncap) : 0;
+            int q = 0;
+            for (unsigned int bits = won; bits; bits &= bits - 1, q++) {
+                int l = __ffs(bits) - 1;
+                unsigned int t = (unsigned int)(c + nb_offset(l, plane, my));
+                if (base != ULLONG_MAX)
                     out[pos++] = hi | (unsigned long long)t;
+                unsigned int sl = slot0 + q;
+                if (sl < kCaptureSlots) {
+                    s_c[sl] = c;
+                    s_t[sl] = t;
+                    s_dom[sl] = (unsigned short)dom;
+                    s_l[sl] = (unsigned char)l;
+                }
+                else {
+                    spill |= 1u << l;
                 }
             }
+            if (won)
+                atomicAdd((unsigned long long *)&desc[dom].liquid_shard[blockIdx.x & (kLiquidShards - 1)],
+                          (unsigned long long)(-(long long)ncap));
         }
-        // set the captured cells active only after their octahedron data is written
-        if (won) {
+        __syncthreads();
+        const unsigned int total = min(s_ncap, (unsigned int)kCaptureSlots);
+        for (unsigned int q = threadIdx.x; q < total; q += kBlock) {
+            const DomainDesc &D = desc[s_dom[q]];
+            capture_cell(D, s_c[q], s_t[q], s_l[q]);
+            // the captured cell becomes active only after its octahedron data is written
+            D.ctype[s_t[q]] = kActive;
+        }
+        for (unsigned int bits = spill; bits; bits &= bits - 1) {
+            int l = __ffs(bits) - 1;
             const DomainDesc &D = desc[dom];
-            int plane = D.mx * D.my;
-            __threadfence();
-            for (unsigned int bits = won; bits; bits &= bits - 1) {
-                int l = __ffs(bits) - 1;
-                long long t = c + (long long)c_nz[l] * plane + c_nx[l] * D.my + c_ny[l];
-                D.ctype[t] = kActive;
-            }
+            unsigned int t = (unsigned int)(c + nb_offset(l, plane, my));
+            capture_cell(D, c, t, l);
+            D.ctype[t] = kActive;
         }
-        long long ncap = __popc(won);
-        warp_add_domain(desc, dom, ncap, &DomainDesc::n_captured);
-        warp_add_liquid(desc, dom, ncap);
-        warp_add_domain(desc, dom, valid ? 1 : 0, &DomainDesc::n_listed);
+        st_captured += ncap;
+        st_kept += keep ? 1 : 0;
+        __syncthreads(); // shared triples are reused by the next iteration
+    }
+    block_stats(P, st_captured, st_kept, kStatCaptured, kStatKept);
+    if (kTail) {
+        __shared__ int s_last;
+        __threadfence(); // this block's writes are visible device-wide before it is counted
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            unsigned int prev = atomicAdd(&P->blocks_done, 1u);
+            s_last = (prev == gridDim.x - 1);
+        }
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            if (threadIdx.x == 0)
+                P->blocks_done = 0;
+            begin_cycle(P);
+        }
     }
 }
 
@@ -610,9 +727,9 @@ __global__ void k_init_active(PoolState *P, int dom, int list_slot) {
         long long c = c0 + threadIdx.x;
         bool act = c < hi && D.ctype[c] == kActive;
         if (act)
-            make_fresh_octahedron(D, c);
+            make_fresh_octahedron(D, (unsigned int)c);
         bool listed = act && c < D.active_size;
-        unsigned long long base = warp_reserve(P, list_slot, listed ? 1u : 0u);
+        unsigned long long base = block_reserve(P, list_slot, listed ? 1u : 0u);
         if (listed && base != ULLONG_MAX)
             P->list[list_slot][base] = ((unsigned long long)dom << 32) | (unsigned long long)c;
     }
@@ -645,6 +762,34 @@ template <class T> T *dalloc(size_t n, std::vector<void *> &allocs, size_t &byte
 }
 } // namespace
 
+void pin_problem(Problem &p) {
+    auto reg = [](void *ptr, size_t bytes) {
+        if (bytes == 0)
+            return;
+        cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
+        if (e != cudaSuccess && e != cudaErrorHostMemoryAlreadyRegistered)
+            throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(e) + " at cudaHostRegister");
+        cudaGetLastError();
+    };
+    reg(p.cell_type.data(), p.cell_type.size());
+    reg(p.grain_id.data(), p.grain_id.size() * 4);
+    reg(p.cts.data(), p.cts.size() * 4);
+    reg(p.layer_id.data(), p.layer_id.size());
+    reg(p.du.data(), p.du.size() * 4);
+    p.pinned = true;
+}
+
+void unpin_problem(Problem &p) {
+    if (!p.pinned)
+        return;
+    for (void *ptr : {(void *)p.cell_type.data(), (void *)p.grain_id.data(), (void *)p.cts.data(),
+                      (void *)p.layer_id.data(), (void *)p.du.data()})
+        if (ptr)
+            cudaHostUnregister(ptr);
+    cudaGetLastError();
+    p.pinned = false;
+}
+
 size_t Pool::slot_bytes(const Problem &p) {
     size_t N = (size_t)p.g.domain_size, A = (size_t)p.g.active_size;
     return N * (1 + 4 + 4 + 1 + 4) + A * (4 + 12 + 104 + 8) + p.nuclei_loc.size() * 8 + 64 * 1024;
@@ -664,8 +809,21 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
     CUDA_OK(cudaMemcpyToSymbol(c_nx, kNeighborX, sizeof(kNeighborX)));
     CUDA_OK(cudaMemcpyToSymbol(c_ny, kNeighborY, sizeof(kNeighborY)));
     CUDA_OK(cudaMemcpyToSymbol(c_nz, kNeighborZ, sizeof(kNeighborZ)));
-    CUDA_OK(cudaMemcpyToSymbol(c_itlist, it, sizeof(it)));
-    CUDA_OK(cudaMemcpyToSymbol(c_itlen, lens, sizeof(lens)));
+    unsigned int itmask[9], zplus = 0, zminus = 0;
+    for (int b = 0; b < 9; b++) {
+        itmask[b] = 0;
+        for (int q = 0; q < lens[b]; q++)
+            itmask[b] |= 1u << it[b][q];
+    }
+    for (int l = 0; l < 26; l++) {
+        if (kNeighborZ[l] == 1)
+            zplus |= 1u << l;
+        if (kNeighborZ[l] == -1)
+            zminus |= 1u << l;
+    }
+    CUDA_OK(cudaMemcpyToSymbol(c_itmask, itmask, sizeof(itmask)));
+    CUDA_OK(cudaMemcpyToSymbol(c_zplus, &zplus, sizeof(zplus)));
+    CUDA_OK(cudaMemcpyToSymbol(c_zminus, &zminus, sizeof(zminus)));
     max_domains_ = 8192;
     capacity_ = std::max<unsigned long long>(list_capacity, 1024);
     CUDA_OK(cudaMalloc(&dstate_, sizeof(PoolState)));
@@ -845,10 +1003,16 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     d.active_size = g.active_size;
     d.du_value = p.du_value;
     long long liquid = 0;
-    for (long i = 0; i < g.domain_size; i++)
-        if (p.cell_type[i] == kLiquid && p.layer_id[i] == 0)
+    int zero_du = 0;
+    for (long i = 0; i < g.domain_size; i++) {
+        int8_t t = p.cell_type[i];
+        if (t == kLiquid && p.layer_id[i] == 0)
             liquid++;
+        if ((t == kLiquid || t == kActive) && p.du[i] == 0.0f)
+            zero_du = 1;
+    }
     d.liquid = liquid;
+    d.zero_du = zero_du;
     host_desc_[slot] = d;
     push_desc(slot);
     ensure_growth(slot, 4096);
@@ -912,9 +1076,39 @@ void Pool::retire(int slot) {
 
 void Pool::launch_step() {
     cudaStream_t st = S(stream_);
-    k_step_begin<<<1, 512, 0, st>>>(dstate_);
-    k_grow_claim<<<num_sms_ * 8, 256, 0, st>>>(dstate_);
-    k_capture<<<num_sms_ * 8, 256, 0, st>>>(dstate_);
+    if (grid_grow_ == 0) {
+        // persistent grids: every resident block slot on the device, grid-stride over the list
+        int b1 = 0, b2 = 0;
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_grow_claim, kBlock, 0));
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_capture<true>, kBlock, 0));
+        grid_grow_ = num_sms_ * std::max(b1, 1);
+        grid_capture_ = num_sms_ * std::max(b2, 1);
+    }
+    k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
+    k_grow_claim<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+    k_capture<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+    launches_ += 3;
+}
+
+// n cycles in one stream sequence: the begin of cycles 2..n runs in the tail of the previous
+// capture kernel, so a cycle costs two launches.
+void Pool::launch_cycles(int n) {
+    if (n <= 0)
+        return;
+    if (grid_grow_ == 0)
+        launch_step(), n--; // sizes the grids on first use
+    if (n <= 0)
+        return;
+    cudaStream_t st = S(stream_);
+    k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
+    launches_ += 1 + 2ull * n;
+    for (int q = 0; q < n; q++) {
+        k_grow_claim<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+        if (q + 1 < n)
+            k_capture<true><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+        else
+            k_capture<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+    }
 }
 
 void Pool::build_graph() {
@@ -923,9 +1117,10 @@ void Pool::build_graph() {
     graph_steps_ = 50;
     cudaStream_t st = S(stream_);
     cudaGraph_t graph;
+    if (grid_grow_ == 0)
+        throw std::runtime_error("grids not sized before graph capture");
     CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    for (int q = 0; q < graph_steps_; q++)
-        launch_step();
+    launch_cycles(graph_steps_);
     CUDA_OK(cudaStreamEndCapture(st, &graph));
     cudaGraphExec_t ex;
     CUDA_OK(cudaGraphInstantiate(&ex, graph, 0));
@@ -936,6 +1131,7 @@ void Pool::build_graph() {
 void Pool::step(int n) {
     if (n <= 0)
         return;
+    cycles_launched_ += (unsigned long long)n;
     CUDA_OK(cudaSetDevice(device_));
     for (int s = 0; s < (int)slots_.size(); s++) {
         if (!slots_[s].used)
@@ -943,13 +1139,17 @@ void Pool::step(int n) {
         slots_[s].steps_launched += n;
         ensure_growth(s, slots_[s].steps_launched + 1);
     }
+    if (grid_grow_ == 0) {
+        launch_step(); // sizes the grids; one cycle
+        n--;
+    }
     build_graph();
     cudaStream_t st = S(stream_);
     int full = n / graph_steps_, rest = n % graph_steps_;
     for (int q = 0; q < full; q++)
         CUDA_OK(cudaGraphLaunch((cudaGraphExec_t)graph_exec_, st));
-    for (int q = 0; q < rest; q++)
-        launch_step();
+    launches_ += (unsigned long long)full * (1 + 2ull * graph_steps_);
+    launch_cycles(rest);
     CUDA_OK(cudaGetLastError());
 }
 
@@ -975,6 +1175,79 @@ unsigned long long Pool::list_count() {
     CUDA_OK(cudaMemcpyAsync(&ps, dstate_, sizeof(ps), cudaMemcpyDeviceToHost, S(stream_)));
     CUDA_OK(cudaStreamSynchronize(S(stream_)));
     return ps.cnt[ps.cur ^ 1];
+}
+
+PoolStats Pool::stats() {
+    PoolState ps;
+    CUDA_OK(cudaMemcpyAsync(&ps, dstate_, sizeof(ps), cudaMemcpyDeviceToHost, S(stream_)));
+    CUDA_OK(cudaStreamSynchronize(S(stream_)));
+    PoolStats r;
+    std::memset(&r, 0, sizeof(r));
+    r.cycles = cycles_launched_;
+    r.launches = launches_;
+    for (int q = 0; q < kStatShards; q++) {
+        r.listed += ps.stat[q][kStatListed];
+        r.grown += ps.stat[q][kStatGrown];
+        r.captured += ps.stat[q][kStatCaptured];
+        r.nucleated += ps.stat[q][kStatNucleated];
+        r.claims += ps.stat[q][kStatClaims];
+        r.liquid_nb += ps.stat[q][kStatLiquidNb];
+        r.kept += ps.stat[q][kStatKept];
+    }
+    return r;
+}
+
+KernelTimes Pool::profile_cycles(int n) {
+    CUDA_OK(cudaSetDevice(device_));
+    KernelTimes kt;
+    if (n <= 0)
+        return kt;
+    if (grid_grow_ == 0) {
+        launch_step();
+        n--;
+        cycles_launched_++;
+    }
+    for (int s = 0; s < (int)slots_.size(); s++) {
+        if (!slots_[s].used)
+            continue;
+        slots_[s].steps_launched += n;
+        ensure_growth(s, slots_[s].steps_launched + 1);
+    }
+    cudaStream_t st = S(stream_);
+    cudaEvent_t ev[4];
+    for (auto &e : ev)
+        CUDA_OK(cudaEventCreate(&e));
+    for (int q = 0; q < n; q++) {
+        CUDA_OK(cudaEventRecord(ev[0], st));
+        k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
+        CUDA_OK(cudaEventRecord(ev[1], st));
+        k_grow_claim<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+        CUDA_OK(cudaEventRecord(ev[2], st));
+        k_capture<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+        CUDA_OK(cudaEventRecord(ev[3], st));
+        CUDA_OK(cudaEventSynchronize(ev[3]));
+        float a, b, c;
+        CUDA_OK(cudaEventElapsedTime(&a, ev[0], ev[1]));
+        CUDA_OK(cudaEventElapsedTime(&b, ev[1], ev[2]));
+        CUDA_OK(cudaEventElapsedTime(&c, ev[2], ev[3]));
+        kt.begin_ms += a;
+        kt.grow_ms += b;
+        kt.capture_ms += c;
+    }
+    for (auto &e : ev)
+        CUDA_OK(cudaEventDestroy(e));
+    kt.cycles = n;
+    cycles_launched_ += n;
+    launches_ += 3ull * n;
+    return kt;
+}
+
+long long Pool::liquid(int slot) const {
+    const DomainDesc &d = host_desc_.at(slot);
+    long long v = d.liquid;
+    for (int q = 0; q < kLiquidShards; q++)
+        v += d.liquid_shard[q];
+    return v;
 }
 
 Census Pool::census(int slot) {
@@ -1049,6 +1322,10 @@ int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_
     const Problem &p = *slots_.at(slot).problem;
     bool jump_type = p.cfg.simulation_type == "S" || p.cfg.simulation_type == "R";
     auto t0 = std::chrono::steady_clock::now();
+    cudaEvent_t ev0, ev1;
+    CUDA_OK(cudaEventCreate(&ev0));
+    CUDA_OK(cudaEventCreate(&ev1));
+    CUDA_OK(cudaEventRecord(ev0, S(stream_)));
     sync_state();
     int cycle = host_desc_[slot].cycle;
     while (true) {
@@ -1081,6 +1358,13 @@ int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_
             }
         }
     }
+    CUDA_OK(cudaEventRecord(ev1, S(stream_)));
+    CUDA_OK(cudaEventSynchronize(ev1));
+    float ms = 0;
+    CUDA_OK(cudaEventElapsedTime(&ms, ev0, ev1));
+    last_run_ms_ = ms;
+    cudaEventDestroy(ev0);
+    cudaEventDestroy(ev1);
     double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     if (nucl_s)
         *nucl_s = 0.0;

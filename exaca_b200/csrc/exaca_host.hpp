@@ -97,6 +97,7 @@ struct Problem {
     double init_seconds = 0.0;
     // baseplate grain centres (x, y, z triples) for the device Voronoi pass of S problems
     std::vector<int32_t> voronoi_seeds;
+    bool pinned = false;
 };
 
 // GrainID placeholder for substrate cells whose Voronoi assignment is computed on the device.
@@ -114,6 +115,10 @@ std::string find_data_file(const std::string &name, const std::string &type, std
 // Builds the geometry, temperature field, substrate, grains and nuclei of a C or S problem
 // (src/CAinitialize.cpp:579-2769). Throws for unsupported problem kinds.
 void initialize_problem(Problem &p, std::string &log);
+
+// Page-locks the per-cell host vectors (cudaHostRegister) for fast admission copies.
+void pin_problem(Problem &p);
+void unpin_problem(Problem &p);
 
 // Host tables derived from the orientation file.
 void read_orientations(const std::string &path, std::vector<float> &guv);

@@ -17,6 +17,19 @@
 namespace exaca {
 
 constexpr int kMaxJumps = 32;
+constexpr int kLiquidShards = 16;
+constexpr int kStatShards = 32;
+// pool statistics, summed over shards
+enum {
+    kStatListed = 0,    // active-list entries visited
+    kStatGrown = 1,     // entries grown (eligible)
+    kStatCaptured = 2,  // captures
+    kStatNucleated = 3, // nucleation events
+    kStatClaims = 4,    // atomicMin claims issued
+    kStatLiquidNb = 5,  // liquid neighbours seen by grown entries
+    kStatKept = 6,      // entries carried into the next list
+    kNumStats = 8
+};
 
 // Device-resident descriptor of one domain. Static fields are written at admission; dynamic
 // fields are advanced by the step kernels and read back by the host.
@@ -42,7 +55,7 @@ struct DomainDesc {
     int check_mode; // 1: the device ends the domain at cycle % 1000 == 0 once no liquid is left
     long long domain_size, active_size;
     float du_value;
-    int pad0;
+    int zero_du; // 1 if a cell that can become active has UndercoolingChange 0 (U stays 0 there)
     // dynamic state
     int cycle;
     unsigned int epoch;
@@ -50,13 +63,11 @@ struct DomainDesc {
     int done;
     int nn;
     int error;
-    long long liquid;
     int n_jumps;
+    long long liquid; // liquid cells of layer 0, less the nucleations (captures are in liquid_shard)
+    long long liquid_shard[kLiquidShards]; // minus the captures, spread over shards to avoid contention
     int jump_lo[kMaxJumps];
     int jump_hi[kMaxJumps];
-    unsigned long long n_grown;    // eligible active-cell updates executed
-    unsigned long long n_captured; // captures executed
-    unsigned long long n_listed;   // list entries visited
 };
 
 // Pool-level device state.
@@ -70,6 +81,20 @@ struct PoolState {
     int n_domains;
     int pad;
     DomainDesc *desc;
+    unsigned long long stat[kStatShards][kNumStats];
+    unsigned int blocks_done; // last-block detection of the capture kernel
+};
+
+struct PoolStats {
+    unsigned long long cycles; // CA cycles launched
+    unsigned long long launches; // kernels launched by step()
+    unsigned long long listed, grown, captured, nucleated, claims, liquid_nb, kept;
+};
+
+// Per-kernel CUDA-event times of a profiled stretch of cycles.
+struct KernelTimes {
+    double begin_ms = 0, grow_ms = 0, capture_ms = 0;
+    int cycles = 0;
 };
 
 // Result of the reference's every-1000-cycle census (src/CAupdate.cpp:738-808).
@@ -120,12 +145,18 @@ class Pool {
     // Reference-equivalent run of one slot to completion with the reference's 1000-cycle census,
     // stdout progress lines and type-S cycle jumps (src/runCA.cpp:290-342).
     int run_plain(int slot, std::string &log, double *nucl_s, double *capture_s);
+    // device time (CUDA events on the pool stream) of the last run_plain
+    double last_run_ms() const { return last_run_ms_; }
+    // runs n cycles with a CUDA event around every kernel (no graph), accumulating their times
+    KernelTimes profile_cycles(int n);
     int n_slots() const { return (int)slots_.size(); }
     bool slot_used(int s) const { return s < (int)slots_.size() && slots_[s].used; }
     size_t bytes_in_use() const { return bytes_in_use_; }
     size_t budget() const { return budget_; }
     int device() const { return device_; }
     unsigned long long list_count();
+    PoolStats stats();
+    long long liquid(int slot) const;
     void set_cycle(int slot, int cycle);
     int pool_error();
 
@@ -133,6 +164,7 @@ class Pool {
     void ensure_growth(int slot, long long needed);
     void push_desc(int slot);
     void launch_step();
+    void launch_cycles(int n);
     void build_graph();
     const DeviceTables &tables_for(const Problem &p);
 
@@ -150,6 +182,10 @@ class Pool {
     std::vector<DomainDesc> host_desc_;
     std::map<std::string, DeviceTables> tables_;
     int num_sms_ = 148;
+    unsigned long long cycles_launched_ = 0;
+    int grid_grow_ = 0, grid_capture_ = 0;
+    unsigned long long launches_ = 0;
+    double last_run_ms_ = 0;
     void *census_buf_ = nullptr;
 };
 

@@ -61,10 +61,20 @@ typedef struct {
     int nn;             /* nucleation events so far */
     int error;          /* device error flags (0 = none) */
     int64_t liquid;     /* liquid cells left */
-    uint64_t n_grown;   /* active-cell growth updates executed */
-    uint64_t n_captured;/* captures executed */
-    uint64_t n_listed;  /* active-list entries visited */
 } exaca_domain_status;
+
+/* Work counters of a pool since its creation (summed over all domains). */
+typedef struct {
+    uint64_t cycles;    /* CA cycles launched */
+    uint64_t launches;  /* kernels launched by exaca_pool_step / run_plain / profile */
+    uint64_t listed;    /* active-list entries visited */
+    uint64_t grown;     /* active cells grown (eligible: cycle > CritTimeStep) */
+    uint64_t captured;  /* liquid cells captured */
+    uint64_t nucleated; /* nucleation events */
+    uint64_t claims;    /* capture claims issued */
+    uint64_t liquid_nb; /* liquid neighbours examined by grown cells */
+    uint64_t kept;      /* list entries carried to the next cycle */
+} exaca_pool_stats_t;
 
 /* The reference's every-1000-cycle census (src/CAupdate.cpp:738-808). */
 typedef struct {
@@ -90,6 +100,8 @@ int exaca_problem_info(const exaca_problem *p, exaca_problem_geometry *info);
  * Voronoi-baseplate cells read INT32_MIN here; the device fills them in at admission. */
 int exaca_problem_fields(const exaca_problem *p, int32_t *cell_type, int32_t *grain_id, int32_t *crit_time_step,
                          float *undercooling_change, int32_t *layer_id);
+/* Page-locks the problem's host fields so that admission copies run at full PCIe bandwidth. */
+int exaca_problem_pin(exaca_problem *p);
 /* Bytes of HBM a problem takes in a pool slot. */
 int64_t exaca_problem_slot_bytes(const exaca_problem *p);
 
@@ -106,12 +118,19 @@ int exaca_pool_admit(exaca_pool *pool, const exaca_problem *p, int device_check,
 int exaca_pool_step(exaca_pool *pool, int n_cycles);
 /* Waits for the device and reads one slot's state. */
 int exaca_pool_status(exaca_pool *pool, int slot, exaca_domain_status *st);
+/* Waits for the device and reads the pool's work counters. */
+int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st);
 /* IntermediateOutputAndCheck's census (src/CAupdate.hpp:30-33) for one slot. */
 int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c);
 /* Runs one slot to completion exactly as the reference's layer loop (src/runCA.cpp:290-342):
  * 1000-cycle census, termination, type-S cycle jump; progress lines are appended to stdout when
  * verbose is 1. */
 int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cycle);
+/* CUDA-event device time (ms) of the last exaca_pool_run_plain on this pool. */
+double exaca_pool_last_run_ms(exaca_pool *pool);
+/* Runs n_cycles cycles kernel by kernel with CUDA events around each launch (no graph) and returns
+ * the summed times in kernel_ms[3] = {cycle start + nucleation, growth + claims, capture + list}. */
+int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms);
 /* Device->host copy of GrainID and CellType (src/runCA.cpp:423-424); NULL skips a field. */
 int exaca_pool_copy_out(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *cell_type);
 /* Active-window octahedron state (DiagonalLength, DOCenter x3, CritDiagonalLength x26). */

@@ -7,7 +7,7 @@ tests/golden/inputs/, and stores per case in tests/golden/<case>.npz:
   init_*       cell fields after initialisation, from the reference's own debug dump (_debug.vtk,
                PrintDebug = 2): CellType, GrainID, CritTimeStep, LayerID, Melted, UndercoolingChange
                on the whole-domain grid (nz, ny, nx) the reference prints
-  final_*      GrainID, CellType (full rank-local arrays) and DiagonalLength at the end of the run,
+  final_*      GrainID and CellType (full rank-local arrays) at the end of the run,
                captured by the shim when the reference releases its views
   sha_*        SHA-256 of the reference's .vtk and _Misorientations.vtk output files, of the final
                DiagonalLength array, and of DOCenter / CritDiagonalLength over cells with DL != 0
@@ -99,7 +99,6 @@ def run_case(case):
             init_du=dbg["UndercoolingChange"].astype(np.float32),
             final_grain_id=gid,
             final_cell_type=ct.astype(np.int8),
-            final_dl=dl,
             sha_vtk=sha(open(os.path.join(work, base + ".vtk"), "rb").read()),
             sha_mis=sha(open(os.path.join(work, base + "_Misorientations.vtk"), "rb").read()),
             sha_dl=sha(dl.tobytes()),
