@@ -73,7 +73,8 @@ class DomainStatus(ctypes.Structure):
 
 class PoolStatsT(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in
-                ("cycles", "launches", "listed", "grown", "captured", "nucleated", "claims", "liquid_nb", "kept")]
+                ("cycles", "launches", "listed", "grown", "captured", "nucleated", "claims", "row_reads", "kept",
+                 "fresh", "rechecks")]
 
 
 class CensusT(ctypes.Structure):

@@ -237,8 +237,10 @@ int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st) {
         st->captured = s.captured;
         st->nucleated = s.nucleated;
         st->claims = s.claims;
-        st->liquid_nb = s.liquid_nb;
+        st->row_reads = s.row_reads;
         st->kept = s.kept;
+        st->fresh = s.fresh;
+        st->rechecks = s.rechecks;
     });
 }
 

@@ -2,18 +2,23 @@
 //
 // One CA cycle (src/runCA.cpp:290-341; src/CAupdate.cpp:67-728) is three kernels over a pool of
 // domains:
-//   k_step_begin   per domain: device-side termination check, cycle/epoch advance, nucleation of
-//                  the sites whose time has come (nuclei are pre-sorted by time, one cursor each).
-//   k_grow_claim   per active cell of the shared compacted list: diagonal-length growth from the
-//                  host-built increment table, then every liquid neighbour it reaches is claimed
-//                  with a 64-bit atomicMin of (epoch, capturer index).
-//   k_capture      per active cell again: each claim it won becomes a capture (new decentred
-//                  octahedron and 26 critical diagonal lengths); it solidifies when no neighbour it
-//                  would have seen as liquid in the reference's serial order remains.
+//   begin (k_step_begin, or the tail of the previous k_resolve): per domain, the device-side
+//          termination check, cycle/epoch advance and nucleation of the sites whose time has come
+//          (nuclei are pre-sorted by time, one cursor each).
+//   k_grow: streams the 16-byte records of the active cells (shared compacted list): diagonal
+//          growth from the host-built increment table, solidification of cells with no liquid
+//          neighbour, and a 64-bit atomicMin claim (epoch, capturer index) on every liquid neighbour
+//          the octahedron reaches. Liquid neighbours come from a per-cell mask kept up to date by
+//          captures and nucleations; the 26 critical lengths are read only when the diagonal has
+//          reached the cached minimum over the liquid neighbours.
+//   k_resolve: one thread per claimed cell: capture by the lowest-index claimant (new decentred
+//          octahedron, 26 critical lengths), mask updates of its active neighbours, and for those
+//          the solidification re-check.
 // The claim rule reproduces the Kokkos-Serial loop order exactly: serial visits active cells in
 // ascending index and captures flip Liquid to Active in place, so the capturer of a cell is the
-// lowest-index claimant and an active cell sees a neighbour as liquid iff it was liquid at the start
-// of the cycle and no lower-index cell claimed it.
+// lowest-index claimant, and an active cell sees a neighbour as liquid iff it was liquid at the
+// start of the cycle and no lower-index cell claimed it. Only cells next to a claimed cell can lose
+// their last such neighbour, so only they are re-checked.
 //
 // Arithmetic follows the reference's types and operation order; this file is compiled with
 // -fmad=false so no multiply-add is contracted, and sqrt/division are IEEE round-to-nearest.
@@ -47,9 +52,13 @@ __constant__ int c_nz[26];
 __constant__ unsigned int c_itmask[9];
 __constant__ unsigned int c_zplus;
 __constant__ unsigned int c_zminus;
+// direction index of a neighbour offset (dz+1)*9 + (dx+1)*3 + (dy+1), and opposite directions
+__constant__ int c_dir[27];
+__constant__ int c_opp[26];
 
-constexpr unsigned int kMaskCarry = 1u << 30; // not eligible this cycle: keep in the list
-constexpr unsigned int kMaskDrop = 1u << 31;  // domain finished: leave the list
+constexpr unsigned int kMaskFresh = 1u << 31; // liquid-neighbour mask not built yet
+constexpr unsigned int kMaskDead = 1u << 30;  // solidified by a re-check: leaves the list next cycle
+constexpr unsigned int kDirBits = (1u << 26) - 1;
 constexpr int kErrGrowthTable = 1;
 constexpr int kErrListOverflow = 2;
 constexpr int kErrBounds = 4;
@@ -72,8 +81,9 @@ __device__ __forceinline__ long long executed_upto(const DomainDesc &D, long lon
     return e;
 }
 
-// Block-aggregated reservation of `n` list slots per thread: one atomicAdd per block. Must be
-// called by every thread of the block. Returns this thread's first slot, or ULLONG_MAX on overflow.
+// Block-aggregated reservation of `n` slots per thread in list `slot`: one atomicAdd per block.
+// Must be called by every thread of the block. Returns this thread's first slot, or ULLONG_MAX on
+// overflow (the pool error flag is set).
 __device__ __forceinline__ unsigned long long block_reserve(PoolState *P, int slot, unsigned int n) {
     __shared__ unsigned int s_warp[kBlock / 32];
     __shared__ unsigned long long s_base;
@@ -115,6 +125,24 @@ __device__ __forceinline__ unsigned long long block_reserve(PoolState *P, int sl
     return r;
 }
 
+// Warp-aggregated reservation (any subset of lanes may call, all with the same counter).
+__device__ __forceinline__ unsigned long long warp_reserve(unsigned long long *counter, unsigned long long cap,
+                                                           int *error) {
+    unsigned int act = __activemask();
+    int lane = threadIdx.x & 31;
+    int leader = __ffs(act) - 1;
+    unsigned long long base = 0;
+    if (lane == leader)
+        base = atomicAdd(counter, (unsigned long long)__popc(act));
+    base = __shfl_sync(act, base, leader);
+    unsigned long long r = base + __popc(act & ((1u << lane) - 1));
+    if (r >= cap) {
+        atomicOr(error, kErrListOverflow);
+        return ULLONG_MAX;
+    }
+    return r;
+}
+
 // Block-level sum of per-thread statistics into one shard of the pool counters.
 __device__ __forceinline__ void block_stats(PoolState *P, unsigned long long a, unsigned long long b, int ia, int ib) {
     __shared__ unsigned long long s_a[kBlock / 32], s_b[kBlock / 32];
@@ -122,6 +150,7 @@ __device__ __forceinline__ void block_stats(PoolState *P, unsigned long long a, 
         a += __shfl_down_sync(0xffffffffu, a, o);
         b += __shfl_down_sync(0xffffffffu, b, o);
     }
+    __syncthreads();
     if ((threadIdx.x & 31) == 0) {
         s_a[threadIdx.x >> 5] = a;
         s_b[threadIdx.x >> 5] = b;
@@ -129,7 +158,7 @@ __device__ __forceinline__ void block_stats(PoolState *P, unsigned long long a, 
     __syncthreads();
     if (threadIdx.x == 0) {
         unsigned long long ta = 0, tb = 0;
-        for (int w = 0; w < kBlock / 32; w++) {
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
             ta += s_a[w];
             tb += s_b[w];
         }
@@ -151,7 +180,9 @@ __device__ __forceinline__ void cell_coords(const DomainDesc &D, unsigned int c,
     ry = (int)(rem - x * (unsigned int)D.my);
 }
 
-// Edge case of src/CAfunctions.cpp:169-213 as a direction mask, restricted to the active window in z.
+// Edge case of src/CAfunctions.cpp:169-213 as a direction mask, restricted to the active window in
+// z (src/CAupdate.cpp:328 checks MyNeighborZ < nzActive; the lower bound never binds for active
+// cells and is kept as a guard).
 __device__ __forceinline__ unsigned int neighbour_mask(const DomainDesc &D, int rx, int ry, int rz) {
     int b = (ry == 0) ? (rx == 0 ? 5 : (rx == D.mx - 1 ? 6 : 1))
                       : (ry == D.my - 1 ? (rx == 0 ? 7 : (rx == D.mx - 1 ? 8 : 2))
@@ -164,9 +195,7 @@ __device__ __forceinline__ unsigned int neighbour_mask(const DomainDesc &D, int 
     return m;
 }
 
-__device__ __forceinline__ long long nb_offset(int l, int plane, int my) {
-    return (long long)c_nz[l] * plane + c_nx[l] * my + c_ny[l];
-}
+__device__ __forceinline__ int nb_offset(int l, int plane, int my) { return c_nz[l] * plane + c_nx[l] * my + c_ny[l]; }
 
 // Fresh octahedron of a newly active cell at its own centre (src/CAupdate.cpp:100-194,
 // src/CAinitialize.cpp:1942-2042): DL = 0.01, centre = cell centre, CDL from the orientation table.
@@ -186,7 +215,9 @@ __device__ void make_fresh_octahedron(const DomainDesc &D, unsigned int c) {
 #pragma unroll
     for (int n = 0; n < 13; n++)
         o[n] = t[n];
+    D.lmask[c] = kMaskFresh;
 }
+
 
 __device__ __forceinline__ long long domain_liquid(const DomainDesc &D) {
     long long v = D.liquid;
@@ -194,179 +225,6 @@ __device__ __forceinline__ long long domain_liquid(const DomainDesc &D) {
     for (int q = 0; q < kLiquidShards; q++)
         v += __ldcg(&D.liquid_shard[q]);
     return v;
-}
-
-// ---------------------------------------------------------------------------------------------
-// Start of a CA cycle for every domain (src/runCA.cpp:290-298, src/CAupdate.cpp:67-200), run by one
-// block: list swap, device-side termination check, cycle advance, nucleation. Reads that may see
-// data other blocks of the same kernel wrote go through L2 (__ldcg).
-__device__ void begin_cycle(PoolState *P) {
-    __shared__ int s_cur;
-    if (threadIdx.x == 0) {
-        // the list built by the previous cycle becomes current; the consumed one is reset
-        int cur = P->cur ^ 1;
-        P->cur = cur;
-        P->cnt[cur ^ 1] = 0;
-        s_cur = cur;
-    }
-    __syncthreads();
-    const int cur = s_cur;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-    unsigned long long nucleated = 0;
-    for (int d = warp; d < P->n_domains; d += nwarps) {
-        DomainDesc &D = P->desc[d];
-        if (D.ctype == nullptr || D.done)
-            continue;
-        if (D.check_mode && D.cycle > 0 && D.cycle % 1000 == 0 && domain_liquid(D) == 0) {
-            // src/CAupdate.cpp:782-783: no superheated or undercooled liquid left
-            if (lane == 0)
-                D.done = 1;
-            continue;
-        }
-        const int cycle = D.cycle + 1;
-        __syncwarp();
-        if (lane == 0) {
-            D.cycle = cycle;
-            D.epoch = D.epoch + 1;
-        }
-        // src/CAupdate.cpp:76-198: sites with cycle >= NucleationTimes that are still liquid
-        int cursor = D.nuc_cursor;
-        int fired_total = 0;
-        while (cursor < D.n_nuclei) {
-            int idx = cursor + lane;
-            int t = idx < D.n_nuclei ? D.nuc_time[idx] : INT_MAX;
-            unsigned int due = __ballot_sync(0xffffffffu, t <= cycle);
-            // nuclei are sorted by time, so the due ones form a prefix
-            int n_due = __popc(due);
-            bool fire = false;
-            unsigned int loc = 0;
-            if (t <= cycle) {
-                int l = D.nuc_loc[idx];
-                if (l < 0 || l >= D.active_size) {
-                    atomicOr(&D.error, kErrBounds);
-                }
-                else {
-                    loc = (unsigned int)l;
-                    fire = __ldcg(D.ctype + loc) == kLiquid && D.layer[loc] <= 0;
-                }
-                if (fire)
-                    make_fresh_octahedron(D, loc);
-            }
-            unsigned int fired = __ballot_sync(0xffffffffu, fire);
-            if (fire) {
-                int rank = __popc(fired & ((1u << lane) - 1));
-                unsigned long long base = 0;
-                if (rank == 0)
-                    base = atomicAdd(&P->cnt[cur], (unsigned long long)__popc(fired));
-                base = __shfl_sync(fired, base, __ffs(fired) - 1);
-                if (base + __popc(fired) > P->capacity)
-                    atomicOr(&P->error, kErrListOverflow);
-                else
-                    P->list[cur][base + rank] = ((unsigned long long)d << 32) | (unsigned long long)loc;
-                D.ctype[loc] = kActive;
-            }
-            fired_total += __popc(fired);
-            cursor += n_due;
-            if (n_due < 32)
-                break;
-        }
-        if (lane == 0) {
-            D.nuc_cursor = cursor;
-            D.nn += fired_total;
-            D.liquid -= fired_total;
-            nucleated += fired_total;
-        }
-    }
-    if (lane == 0 && nucleated)
-        atomicAdd(&P->stat[0][kStatNucleated], nucleated);
-}
-
-__global__ void k_step_begin(PoolState *P) { begin_cycle(P); }
-
-// ---------------------------------------------------------------------------------------------
-// k_grow_claim: src/CAupdate.cpp:217-352 for every listed active cell
-__global__ void __launch_bounds__(kBlock) k_grow_claim(PoolState *P) {
-    const int cur = P->cur;
-    const unsigned long long n = P->cnt[cur];
-    const unsigned long long *list = P->list[cur];
-    unsigned int *mask = P->mask;
-    DomainDesc *desc = P->desc;
-    const unsigned long long stride = (unsigned long long)gridDim.x * kBlock;
-    unsigned long long st_listed = 0, st_grown = 0, st_claims = 0, st_liq = 0;
-    for (unsigned long long i = (unsigned long long)blockIdx.x * kBlock + threadIdx.x; i < n; i += stride) {
-        unsigned long long e = list[i];
-        unsigned int dom = (unsigned int)(e >> 32);
-        unsigned int c = (unsigned int)e;
-        DomainDesc &D = desc[dom];
-        st_listed++;
-        unsigned int m;
-        if (D.done) {
-            m = kMaskDrop;
-        }
-        else {
-            const int cycle = D.cycle;
-            const int cts = D.cts[c];
-            // single-layer problems only (checked at admission): LayerID <= layer always holds
-            if (!(cycle > cts)) {
-                m = kMaskCarry;
-            }
-            else {
-                st_grown++;
-                // undercooling after the executed updates since the liquidus (src/CAupdate.cpp:236-237)
-                long long nu = executed_upto(D, cycle) - executed_upto(D, cts);
-                if (D.zero_du && D.du[c] == 0.0f)
-                    nu = 0;
-                double inc = 0.0;
-                if (nu >= 0 && nu < D.growth_len)
-                    inc = __ldg(D.growth + nu);
-                else
-                    atomicOr(&D.error, kErrGrowthTable);
-                const float dl = (float)((double)D.dl[c] + inc);
-                D.dl[c] = dl;
-                int rx, ry, rz;
-                cell_coords(D, c, rx, ry, rz);
-                const unsigned int valid = neighbour_mask(D, rx, ry, rz);
-                const int plane = D.mx * D.my, my = D.my;
-                const int8_t *ct = D.ctype + c;
-                // the 26 critical lengths as 13 aligned 8-byte loads (26 * 4 * c is 8-byte aligned),
-                // issued together with the 26 independent neighbour-type loads
-                const float2 *row = reinterpret_cast<const float2 *>(D.cdl + 26ull * c);
-                float cdl[26];
-#pragma unroll
-                for (int q = 0; q < 13; q++) {
-                    float2 v = row[q];
-                    cdl[2 * q] = v.x;
-                    cdl[2 * q + 1] = v.y;
-                }
-                unsigned int liq = 0;
-#pragma unroll
-                for (int l = 0; l < 26; l++) {
-                    if (valid & (1u << l)) {
-                        if (ct[nb_offset(l, plane, my)] == kLiquid)
-                            liq |= 1u << l;
-                    }
-                }
-                if (liq) {
-                    const unsigned long long key =
-                        ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
-                    unsigned long long *claim = D.claim + c;
-#pragma unroll
-                    for (int l = 0; l < 26; l++) {
-                        if ((liq & (1u << l)) && dl >= cdl[l]) {
-                            atomicMin(claim + nb_offset(l, plane, my), key);
-                            st_claims++;
-                        }
-                    }
-                }
-                st_liq += __popc(liq);
-                m = liq;
-            }
-        }
-        mask[i] = m;
-    }
-    block_stats(P, st_listed, st_grown, kStatListed, kStatGrown);
-    __syncthreads();
-    block_stats(P, st_claims, st_liq, kStatClaims, kStatLiquidNb);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -491,126 +349,498 @@ __device__ void capture_cell(const DomainDesc &D, long long c, long long t, int 
     }
 }
 
-// k_capture: captures won, solidification (src/CAupdate.cpp:336-352, 722-725), next list.
-// The capture geometry (a long double-precision dependency chain) is spread over the block: every
-// won (capturer, target, direction) triple goes to shared memory and the block's threads take one
-// each. With kTail the last block to finish also starts the next cycle (begin_cycle).
-constexpr int kCaptureSlots = 1024;
-
-template <bool kTail> __global__ void __launch_bounds__(kBlock) k_capture(PoolState *P) {
-    __shared__ unsigned int s_c[kCaptureSlots], s_t[kCaptureSlots];
-    __shared__ unsigned short s_dom[kCaptureSlots];
-    __shared__ unsigned char s_l[kCaptureSlots];
-    __shared__ unsigned int s_ncap;
-    const int cur = P->cur;
-    const int nxt = cur ^ 1;
-    const unsigned long long n = P->cnt[cur];
-    const unsigned long long *list = P->list[cur];
-    unsigned long long *out = P->list[nxt];
-    const unsigned int *mask = P->mask;
-    DomainDesc *desc = P->desc;
-    const unsigned long long stride = (unsigned long long)gridDim.x * kBlock;
-    unsigned long long st_captured = 0, st_kept = 0;
-    // block-uniform loop so that block_reserve is reached by every thread
-    for (unsigned long long i0 = (unsigned long long)blockIdx.x * kBlock; i0 < n; i0 += stride) {
-        const unsigned long long i = i0 + threadIdx.x;
-        const bool valid = i < n;
-        unsigned long long e = 0;
-        unsigned int m = kMaskDrop;
-        if (valid) {
-            e = list[i];
-            m = mask[i];
-        }
-        const unsigned int dom = (unsigned int)(e >> 32);
-        const unsigned int c = (unsigned int)e;
-        unsigned int won = 0;
-        bool keep = false;
-        int plane = 0, my = 0;
-        if (!(m & kMaskDrop)) {
-            if (m & kMaskCarry) {
-                keep = true;
-            }
-            else {
-                const DomainDesc &D = desc[dom];
-                plane = D.mx * D.my;
-                my = D.my;
-                const unsigned int want = 0xffffffffu - D.epoch;
-                const unsigned long long *claim = D.claim + c;
-                bool lcount = false;
+// Does active cell a still see a liquid neighbour at the end of this cycle's serial order? Its
+// neighbours that were liquid at the start of the cycle are the claimed ones plus the unclaimed
+// bits of its mask (only captures clear mask bits, and every capture was claimed). Captured by a
+// lower index = seen as active; otherwise seen as liquid (src/CAupdate.cpp:333-334, 722-725).
+// All 26 claim words are loaded before any is examined.
+__device__ bool still_sees_liquid(const DomainDesc &D, unsigned int a) {
+    int rx, ry, rz;
+    cell_coords(D, a, rx, ry, rz);
+    const unsigned int valid = neighbour_mask(D, rx, ry, rz);
+    const unsigned int m = __ldcg(D.lmask + a);
+    const unsigned int want = 0xffffffffu - D.epoch;
+    const int plane = D.mx * D.my, my = D.my;
+    const unsigned long long *claim = D.claim + a;
+    unsigned long long k[26];
 #pragma unroll
-                for (int l = 0; l < 26; l++) {
-                    if (m & (1u << l)) {
-                        unsigned long long k = claim[nb_offset(l, plane, my)];
-                        if ((unsigned int)(k >> 32) == want) {
-                            unsigned int w = (unsigned int)k;
-                            if (w >= c)
-                                lcount = true;
-                            if (w == c)
-                                won |= 1u << l;
-                        }
-                        else {
-                            lcount = true;
-                        }
-                    }
-                }
-                if (!lcount)
-                    D.ctype[c] = kSolid;
-                keep = lcount;
-            }
+    for (int l = 0; l < 26; l++)
+        k[l] = (valid & (1u << l)) ? __ldcg(claim + nb_offset(l, plane, my)) : 0ull;
+    bool sees = false;
+#pragma unroll
+    for (int l = 0; l < 26; l++) {
+        if (valid & (1u << l)) {
+            if ((unsigned int)(k[l] >> 32) == want)
+                sees |= (unsigned int)k[l] >= a;
+            else
+                sees |= (m >> l) & 1u;
         }
-        const unsigned int ncap = (unsigned int)__popc(won);
-        const unsigned int n_out = (keep ? 1u : 0u) + ncap;
-        if (threadIdx.x == 0)
-            s_ncap = 0;
-        const unsigned long long base = block_reserve(P, nxt, n_out);
-        unsigned int spill = 0; // triples that do not fit in shared memory stay with this thread
-        if (n_out) {
-            unsigned long long pos = base;
-            if (keep && base != ULLONG_MAX)
-                out[pos++] = e;
-            const unsigned long long hi = (unsigned long long)dom << 32;
-            unsigned int slot0 = ncap ? atomicAdd(&s_ncap, ncap) : 0;
-            int q = 0;
-            for (unsigned int bits = won; bits; bits &= bits - 1, q++) {
-                int l = __ffs(bits) - 1;
-                unsigned int t = (unsigned int)(c + nb_offset(l, plane, my));
-                if (base != ULLONG_MAX)
-                    out[pos++] = hi | (unsigned long long)t;
-                unsigned int sl = slot0 + q;
-                if (sl < kCaptureSlots) {
-                    s_c[sl] = c;
-                    s_t[sl] = t;
-                    s_dom[sl] = (unsigned short)dom;
-                    s_l[sl] = (unsigned char)l;
+    }
+    return sees;
+}
+
+// A nucleation site stopped being liquid: its active neighbours drop it from their masks.
+__device__ void drop_from_neighbour_masks(const DomainDesc &D, unsigned int t) {
+    int rx, ry, rz;
+    cell_coords(D, t, rx, ry, rz);
+    const unsigned int valid = neighbour_mask(D, rx, ry, rz);
+    const int plane = D.mx * D.my, my = D.my;
+    for (unsigned int bits = valid; bits; bits &= bits - 1) {
+        int l = __ffs(bits) - 1;
+        unsigned int a = (unsigned int)((long long)t + nb_offset(l, plane, my));
+        if (__ldcg(D.ctype + a) == kActive)
+            atomicAnd(D.lmask + a, ~(1u << c_opp[l]));
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Start of a CA cycle for every domain (src/runCA.cpp:290-298, src/CAupdate.cpp:67-200), run by one
+// block: list swap, device-side termination check, cycle advance, nucleation. Reads that may see
+// data other blocks of the same kernel wrote go through L2 (__ldcg).
+__device__ void begin_cycle(PoolState *P) {
+    __shared__ int s_cur;
+    if (threadIdx.x == 0) {
+        // the list the previous cycle left becomes current; when it was a compacted copy, the old
+        // one is emptied and carries no dropped records any more
+        int prev = P->cur;
+        int cur = P->pending;
+        if (cur != prev) {
+            P->cnt[prev] = 0;
+            P->tombs = 0;
+        }
+        P->cur = cur;
+        // compact when dropped records exceed an eighth of the list
+        int compact = P->tombs * 8 > P->cnt[cur] ? 1 : 0;
+        P->compact = compact;
+        P->pending = compact ? cur ^ 1 : cur;
+        if (compact)
+            P->cnt[cur ^ 1] = 0;
+        P->tcnt = 0;
+        P->work[0] = 0;
+        P->work[1] = 0;
+        s_cur = cur;
+    }
+    __syncthreads();
+    const int cur = s_cur;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+    unsigned long long nucleated = 0;
+    for (int d = warp; d < P->n_domains; d += nwarps) {
+        DomainDesc &D = P->desc[d];
+        if (D.ctype == nullptr || D.done)
+            continue;
+        if (D.check_mode && D.cycle > 0 && D.cycle % 1000 == 0 && domain_liquid(D) == 0) {
+            // src/CAupdate.cpp:782-783: no superheated or undercooled liquid left
+            if (lane == 0)
+                D.done = 1;
+            continue;
+        }
+        const int cycle = D.cycle + 1;
+        __syncwarp();
+        if (lane == 0) {
+            D.cycle = cycle;
+            D.epoch = D.epoch + 1;
+        }
+        // src/CAupdate.cpp:76-198: sites with cycle >= NucleationTimes that are still liquid
+        int cursor = D.nuc_cursor;
+        int fired_total = 0;
+        while (cursor < D.n_nuclei) {
+            int idx = cursor + lane;
+            int t = idx < D.n_nuclei ? D.nuc_time[idx] : INT_MAX;
+            unsigned int due = __ballot_sync(0xffffffffu, t <= cycle);
+            // nuclei are sorted by time, so the due ones form a prefix
+            int n_due = __popc(due);
+            bool fire = false;
+            unsigned int loc = 0;
+            if (t <= cycle) {
+                int l = D.nuc_loc[idx];
+                if (l < 0 || l >= D.active_size) {
+                    atomicOr(&D.error, kErrBounds);
                 }
                 else {
-                    spill |= 1u << l;
+                    loc = (unsigned int)l;
+                    fire = __ldcg(D.ctype + loc) == kLiquid && D.layer[loc] <= 0;
                 }
             }
-            if (won)
-                atomicAdd((unsigned long long *)&desc[dom].liquid_shard[blockIdx.x & (kLiquidShards - 1)],
-                          (unsigned long long)(-(long long)ncap));
+            if (fire) {
+                make_fresh_octahedron(D, loc);
+                unsigned long long pos = warp_reserve(&P->cnt[cur], P->capacity, &P->error);
+                if (pos != ULLONG_MAX) {
+                    ActiveRec r;
+                    r.cell = loc;
+                    r.dl = 0.01f;
+                    r.cdl_min = 0.0f;
+                    r.cts = D.cts[loc];
+                    P->rec[cur][pos] = r;
+                    P->rdom[cur][pos] = (unsigned int)d;
+                }
+                D.ctype[loc] = kActive;
+            }
+            __syncwarp();
+            if (fire)
+                drop_from_neighbour_masks(D, loc);
+            unsigned int fired = __ballot_sync(0xffffffffu, fire);
+            fired_total += __popc(fired);
+            cursor += n_due;
+            if (n_due < 32)
+                break;
         }
-        __syncthreads();
-        const unsigned int total = min(s_ncap, (unsigned int)kCaptureSlots);
-        for (unsigned int q = threadIdx.x; q < total; q += kBlock) {
-            const DomainDesc &D = desc[s_dom[q]];
-            capture_cell(D, s_c[q], s_t[q], s_l[q]);
-            // the captured cell becomes active only after its octahedron data is written
-            D.ctype[s_t[q]] = kActive;
+        if (lane == 0) {
+            D.nuc_cursor = cursor;
+            D.nn += fired_total;
+            D.liquid -= fired_total;
+            nucleated += fired_total;
         }
-        for (unsigned int bits = spill; bits; bits &= bits - 1) {
-            int l = __ffs(bits) - 1;
-            const DomainDesc &D = desc[dom];
-            unsigned int t = (unsigned int)(c + nb_offset(l, plane, my));
-            capture_cell(D, c, t, l);
-            D.ctype[t] = kActive;
-        }
-        st_captured += ncap;
-        st_kept += keep ? 1 : 0;
-        __syncthreads(); // shared triples are reused by the next iteration
     }
-    block_stats(P, st_captured, st_kept, kStatCaptured, kStatKept);
+    if (lane == 0 && nucleated)
+        atomicAdd(&P->stat[0][kStatNucleated], nucleated);
+}
+
+__global__ void k_step_begin(PoolState *P) { begin_cycle(P); }
+
+// ---------------------------------------------------------------------------------------------
+// Per-cycle growth of the active cells, split by cost:
+//   k_grow    streams every record (kBatch per thread, loads issued first): eligibility, diagonal
+//             growth (src/CAupdate.cpp:257-261), drop of finished / re-check-solidified cells, and
+//             solidification of cells whose liquid mask is empty. A record whose mask must still
+//             be built, or whose diagonal reached the cached minimum critical length, is flagged
+//             (cdl_min = kNeedsClaim) for
+//   k_claim   one thread per flagged record, chunks handed out dynamically: the liquid mask from
+//             the 26 neighbour types, the critical-length row (13 aligned 8-byte loads), and the
+//             claims (src/CAupdate.cpp:320-352).
+constexpr unsigned int kNeedsClaim = 0xffffffffu; // NaN pattern in ActiveRec::cdl_min
+constexpr int kBatch = 4;
+
+struct GrowStats {
+    unsigned long long listed = 0, grown = 0, dropped = 0, flagged = 0;
+};
+
+// Growth step of one record with its liquid mask and growth increment loaded. Returns 0: drop
+// the record, 1: keep it unchanged (not eligible yet), 2: keep the updated record.
+__device__ __forceinline__ int grow_record(DomainDesc &D, ActiveRec &r, unsigned int m, double inc, bool inc_ok,
+                                           GrowStats &st) {
+    const unsigned int c = r.cell;
+    st.listed++;
+    if (D.done || (m & kMaskDead)) {
+        // finished domain, or solidified by last cycle's re-check
+        D.dl[c] = r.dl;
+        return 0;
+    }
+    if (!(D.cycle > r.cts))
+        return 1; // single-layer problems only: LayerID <= layer always holds
+    st.grown++;
+    if (!inc_ok)
+        atomicOr(&D.error, kErrGrowthTable);
+    const float dl = (float)((double)r.dl + inc);
+    r.dl = dl;
+    if ((m & kMaskFresh) || dl >= r.cdl_min) {
+        r.cdl_min = __uint_as_float(kNeedsClaim);
+        st.flagged++;
+        return 2;
+    }
+    if (m == 0) {
+        // no liquid neighbour: LCount stays 0 (src/CAupdate.cpp:722-725)
+        D.ctype[c] = kSolid;
+        D.dl[c] = dl;
+        return 0;
+    }
+    return 2;
+}
+
+__device__ __forceinline__ void load_growth(const DomainDesc &D, const ActiveRec &r, unsigned int &m, double &inc,
+                                            bool &ok) {
+    m = D.lmask[r.cell];
+    // undercooling after the executed updates since the liquidus (src/CAupdate.cpp:236-237)
+    long long nu = executed_upto(D, D.cycle) - executed_upto(D, r.cts);
+    if (D.zero_du && D.du[r.cell] == 0.0f)
+        nu = 0;
+    ok = nu >= 0 && nu < D.growth_len;
+    inc = (ok && D.cycle > r.cts) ? __ldg(D.growth + nu) : 0.0;
+}
+
+__global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
+    const int cur = P->cur;
+    const unsigned long long n = P->cnt[cur];
+    ActiveRec *in = P->rec[cur];
+    const unsigned int *in_dom = P->rdom[cur];
+    DomainDesc *desc = P->desc;
+    GrowStats st;
+    if (!P->compact) {
+        // records are updated in place; dropped ones become tombstones
+        const unsigned long long step = (unsigned long long)gridDim.x * kBlock * kBatch;
+        for (unsigned long long base = (unsigned long long)blockIdx.x * kBlock * kBatch + threadIdx.x; base < n;
+             base += step) {
+            ActiveRec r[kBatch];
+            unsigned int dom[kBatch], m[kBatch];
+            double inc[kBatch];
+            bool ok[kBatch];
+#pragma unroll
+            for (int q = 0; q < kBatch; q++) {
+                const unsigned long long i = base + (unsigned long long)q * kBlock;
+                r[q].cell = kTombstone;
+                dom[q] = 0;
+                if (i < n) {
+                    r[q] = in[i];
+                    dom[q] = in_dom[i];
+                }
+            }
+#pragma unroll
+            for (int q = 0; q < kBatch; q++) {
+                m[q] = 0;
+                inc[q] = 0.0;
+                ok[q] = true;
+                if (r[q].cell != kTombstone)
+                    load_growth(desc[dom[q]], r[q], m[q], inc[q], ok[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < kBatch; q++) {
+                if (r[q].cell == kTombstone)
+                    continue;
+                const unsigned long long i = base + (unsigned long long)q * kBlock;
+                const int a = grow_record(desc[dom[q]], r[q], m[q], inc[q], ok[q], st);
+                if (a == 0) {
+                    ActiveRec tomb = r[q];
+                    tomb.cell = kTombstone;
+                    tomb.cdl_min = 0.0f;
+                    in[i] = tomb;
+                    st.dropped++;
+                }
+                else if (a == 2) {
+                    *reinterpret_cast<float2 *>(&in[i].dl) = make_float2(r[q].dl, r[q].cdl_min);
+                }
+            }
+        }
+    }
+    else {
+        // compaction: the survivors are written to the other list
+        const int nxt = cur ^ 1;
+        ActiveRec *out = P->rec[nxt];
+        unsigned int *out_dom = P->rdom[nxt];
+        const unsigned long long stride = (unsigned long long)gridDim.x * kBlock;
+        // block-uniform loop: block_reserve is reached by every thread
+        for (unsigned long long i0 = (unsigned long long)blockIdx.x * kBlock; i0 < n; i0 += stride) {
+            const unsigned long long i = i0 + threadIdx.x;
+            bool keep = false;
+            ActiveRec r;
+            unsigned int dom = 0;
+            if (i < n) {
+                r = in[i];
+                dom = in_dom[i];
+                if (r.cell != kTombstone) {
+                    unsigned int m;
+                    double inc;
+                    bool ok;
+                    load_growth(desc[dom], r, m, inc, ok);
+                    keep = grow_record(desc[dom], r, m, inc, ok, st) != 0;
+                }
+            }
+            const unsigned long long pos = block_reserve(P, nxt, keep ? 1u : 0u);
+            if (keep && pos != ULLONG_MAX) {
+                out[pos] = r;
+                out_dom[pos] = dom;
+            }
+        }
+    }
+    block_stats(P, st.listed, st.grown, kStatListed, kStatGrown);
+    block_stats(P, st.dropped, st.flagged, kStatDropped, kStatFlagged);
+    if (!P->compact) {
+        // dropped records stay as tombstones until the next compaction
+        __shared__ unsigned long long s_d;
+        if (threadIdx.x == 0)
+            s_d = 0;
+        __syncthreads();
+        if (st.dropped)
+            atomicAdd(&s_d, st.dropped);
+        __syncthreads();
+        if (threadIdx.x == 0 && s_d)
+            atomicAdd(&P->tombs, s_d);
+    }
+}
+
+// Next chunk of kBlock work items for this block, handed out by an atomic counter.
+__device__ __forceinline__ unsigned long long next_chunk(unsigned long long *counter) {
+    __shared__ unsigned long long s_chunk;
+    __syncthreads();
+    if (threadIdx.x == 0)
+        s_chunk = atomicAdd(counter, 1ull);
+    __syncthreads();
+    return s_chunk;
+}
+
+__global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
+    const int lst = P->pending; // the list the growth pass just wrote
+    const unsigned long long n = P->cnt[lst];
+    ActiveRec *recs = P->rec[lst];
+    const unsigned int *rdom = P->rdom[lst];
+    DomainDesc *desc = P->desc;
+    unsigned long long st_claims = 0, st_rows = 0, st_fresh = 0, st_dropped = 0;
+    for (;;) {
+        const unsigned long long chunk = next_chunk(&P->work[0]);
+        const unsigned long long i = chunk * kBlock + threadIdx.x;
+        if (chunk * kBlock >= n)
+            break;
+        if (i >= n)
+            continue;
+        const ActiveRec rec = recs[i];
+        if (rec.cell == kTombstone || __float_as_uint(rec.cdl_min) != kNeedsClaim)
+            continue;
+        const unsigned int c = rec.cell;
+        const unsigned int dom = rdom[i];
+        DomainDesc &D = desc[dom];
+        const float dl = rec.dl;
+        const int plane = D.mx * D.my, my = D.my;
+        int rx, ry, rz;
+        cell_coords(D, c, rx, ry, rz);
+        unsigned int m = D.lmask[c];
+        if (m & kMaskFresh) {
+            // liquid neighbours from the 26 neighbour types (src/CAupdate.cpp:320-334); no other
+            // thread writes this cell's mask now, captures and nucleations clear bits later
+            st_fresh++;
+            const unsigned int valid = neighbour_mask(D, rx, ry, rz);
+            const int8_t *ct = D.ctype + c;
+            m = 0;
+#pragma unroll
+            for (int l = 0; l < 26; l++)
+                if ((valid & (1u << l)) && ct[nb_offset(l, plane, my)] == kLiquid)
+                    m |= 1u << l;
+            D.lmask[c] = m;
+        }
+        if (m == 0) {
+            // no liquid neighbour: LCount stays 0 (src/CAupdate.cpp:722-725)
+            D.ctype[c] = kSolid;
+            D.dl[c] = dl;
+            ActiveRec tomb = rec;
+            tomb.cell = kTombstone;
+            tomb.cdl_min = 0.0f;
+            recs[i] = tomb;
+            st_dropped++;
+            continue;
+        }
+        // the 26 critical lengths as 13 aligned 8-byte loads (26 * 4 * c is 8-byte aligned)
+        st_rows++;
+        const float2 *row = reinterpret_cast<const float2 *>(D.cdl + 26ull * c);
+        float cdl[26];
+#pragma unroll
+        for (int q = 0; q < 13; q++) {
+            float2 v = row[q];
+            cdl[2 * q] = v.x;
+            cdl[2 * q + 1] = v.y;
+        }
+        float nm = __int_as_float(0x7f800000);
+        unsigned int reach = 0;
+#pragma unroll
+        for (int l = 0; l < 26; l++) {
+            if (m & (1u << l)) {
+                nm = (cdl[l] < nm) ? cdl[l] : nm;
+                if (dl >= cdl[l])
+                    reach |= 1u << l;
+            }
+        }
+        recs[i].cdl_min = nm;
+        if (reach) {
+            // claims (src/CAupdate.cpp:336-352): lowest index wins; the first claimant of a cell in
+            // this cycle lists it for k_resolve
+            const unsigned long long key = ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
+            const unsigned int want = 0xffffffffu - D.epoch;
+            unsigned int first = 0;
+#pragma unroll
+            for (int l = 0; l < 26; l++) {
+                if (reach & (1u << l)) {
+                    unsigned long long old = atomicMin(D.claim + (long long)c + nb_offset(l, plane, my), key);
+                    if ((unsigned int)(old >> 32) != want)
+                        first |= 1u << l;
+                }
+            }
+            st_claims += __popc(reach);
+            for (unsigned int bits = first; bits; bits &= bits - 1) {
+                int l = __ffs(bits) - 1;
+                unsigned long long pos = warp_reserve(&P->tcnt, P->capacity, &P->error);
+                if (pos != ULLONG_MAX)
+                    P->tgt[pos] = ((unsigned long long)dom << 32) | (unsigned int)((long long)c + nb_offset(l, plane, my));
+            }
+        }
+    }
+    block_stats(P, st_claims, st_rows, kStatClaims, kStatRowReads);
+    block_stats(P, st_fresh, 0, kStatFresh, kStatFresh);
+    if (st_dropped && !P->compact)
+        atomicAdd(&P->tombs, st_dropped);
+}
+
+// k_resolve: every cell claimed this cycle is captured by its lowest-index claimant
+// (src/CAupdate.cpp:336-563, 713-717), its active neighbours drop it from their liquid masks, and
+// those grown this cycle re-check whether they still see a liquid neighbour
+// (src/CAupdate.cpp:722-725). Work items (captures first, then 26 neighbour updates per claimed
+// cell) are handed out in chunks. With kTail the last block to finish starts the next cycle.
+template <bool kTail> __global__ void __launch_bounds__(kBlock) k_resolve(PoolState *P) {
+    const int app = P->pending; // list of the next cycle
+    const unsigned long long T = P->tcnt;
+    const unsigned long long n = T * 27ull;
+    DomainDesc *desc = P->desc;
+    unsigned long long st_cap = 0, st_rc = 0;
+    for (;;) {
+        const unsigned long long chunk = next_chunk(&P->work[1]);
+        if (chunk * kBlock >= n)
+            break;
+        const unsigned long long j = chunk * kBlock + threadIdx.x;
+        if (j >= n)
+            continue;
+        if (j < T) {
+            const unsigned long long e = P->tgt[j];
+            const unsigned int dom = (unsigned int)(e >> 32);
+            const unsigned int t = (unsigned int)e;
+            DomainDesc &D = desc[dom];
+            const unsigned int w = (unsigned int)__ldcg(D.claim + t);
+            int wx, wy, wz, tx, ty, tz;
+            cell_coords(D, w, wx, wy, wz);
+            cell_coords(D, t, tx, ty, tz);
+            const int l = c_dir[(tz - wz + 1) * 9 + (tx - wx + 1) * 3 + (ty - wy + 1)];
+            capture_cell(D, w, t, l);
+            D.lmask[t] = kMaskFresh;
+            unsigned long long pos = warp_reserve(&P->cnt[app], P->capacity, &P->error);
+            if (pos != ULLONG_MAX) {
+                ActiveRec r;
+                r.cell = t;
+                r.dl = __ldcg(D.dl + t);
+                r.cdl_min = 0.0f;
+                r.cts = __ldg(D.cts + t);
+                P->rec[app][pos] = r;
+                P->rdom[app][pos] = dom;
+            }
+            // the captured cell becomes active only after its octahedron data is written
+            D.ctype[t] = kActive;
+            atomicAdd((unsigned long long *)&D.liquid_shard[blockIdx.x & (kLiquidShards - 1)],
+                      (unsigned long long)(-1ll));
+            st_cap++;
+        }
+        else {
+            // neighbour a of a claimed cell t: drop t from a's liquid mask; a cell grown this
+            // cycle re-checks whether it still sees a liquid neighbour
+            const unsigned long long q = (j - T) / 26ull;
+            const int l = (int)((j - T) - q * 26ull);
+            const unsigned long long e = P->tgt[q];
+            const unsigned int dom = (unsigned int)(e >> 32);
+            const unsigned int t = (unsigned int)e;
+            DomainDesc &D = desc[dom];
+            int tx, ty, tz;
+            cell_coords(D, t, tx, ty, tz);
+            if (!(neighbour_mask(D, tx, ty, tz) & (1u << l)))
+                continue;
+            const unsigned int a = (unsigned int)((long long)t + nb_offset(l, D.mx * D.my, D.my));
+            if (__ldcg(D.ctype + a) != kActive)
+                continue;
+            // the mask bits of claimed cells do not matter to the re-check, so the clear need not
+            // complete first
+            atomicAnd(D.lmask + a, ~(1u << c_opp[l]));
+            const unsigned int m = __ldcg(D.lmask + a);
+            if (!(m & (kMaskFresh | kMaskDead)) && D.cycle > __ldg(D.cts + a)) {
+                st_rc++;
+                if (!still_sees_liquid(D, a)) {
+                    D.ctype[a] = kSolid;
+                    atomicOr(D.lmask + a, kMaskDead);
+                }
+            }
+        }
+    }
+    block_stats(P, st_cap, st_rc, kStatCaptured, kStatRechecks);
     if (kTail) {
         __shared__ int s_last;
         __threadfence(); // this block's writes are visible device-wide before it is counted
@@ -714,7 +944,7 @@ __global__ void k_voronoi(DomainDesc *Dp, const int32_t *seeds, int nseeds, floa
         D.gid[c] = best_i + 1;
 }
 
-// Initially active cells: fresh octahedra and the first active list (src/CAinitialize.cpp:1929-2044).
+// Initially active cells: fresh octahedra and the first records (src/CAinitialize.cpp:1929-2044).
 __global__ void k_init_active(PoolState *P, int dom, int list_slot) {
     DomainDesc &D = P->desc[dom];
     long long plane = (long long)D.mx * D.my;
@@ -729,22 +959,42 @@ __global__ void k_init_active(PoolState *P, int dom, int list_slot) {
         if (act)
             make_fresh_octahedron(D, (unsigned int)c);
         bool listed = act && c < D.active_size;
-        unsigned long long base = block_reserve(P, list_slot, listed ? 1u : 0u);
-        if (listed && base != ULLONG_MAX)
-            P->list[list_slot][base] = ((unsigned long long)dom << 32) | (unsigned long long)c;
+        unsigned long long pos = block_reserve(P, list_slot, listed ? 1u : 0u);
+        if (listed && pos != ULLONG_MAX) {
+            ActiveRec r;
+            r.cell = (unsigned int)c;
+            r.dl = 0.01f;
+            r.cdl_min = 0.0f;
+            r.cts = D.cts[c];
+            P->rec[list_slot][pos] = r;
+            P->rdom[list_slot][pos] = (unsigned int)dom;
+        }
     }
 }
 
-// Re-labels every entry of one domain in the list the next cycle consumes with the pool's
+// Re-labels every record of one domain in the list the next cycle consumes with the pool's
 // always-finished placeholder domain (used when a slot is retired, before the slot is reused).
 __global__ void k_drop_domain(PoolState *P, unsigned int dom, unsigned int placeholder) {
-    const int nxt = P->cur ^ 1;
+    const int nxt = P->pending;
     unsigned long long n = P->cnt[nxt];
-    unsigned long long *list = P->list[nxt];
+    unsigned int *d = P->rdom[nxt];
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (unsigned long long)gridDim.x * blockDim.x)
-        if ((unsigned int)(list[i] >> 32) == dom)
-            list[i] = (unsigned long long)placeholder << 32;
+        if (d[i] == dom)
+            d[i] = placeholder;
+}
+
+// Diagonal lengths held in the pending records back to the per-cell arrays.
+__global__ void k_flush_records(PoolState *P) {
+    const int nxt = P->pending;
+    unsigned long long n = P->cnt[nxt];
+    for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+         i += (unsigned long long)gridDim.x * blockDim.x) {
+        const ActiveRec r = P->rec[nxt][i];
+        const DomainDesc &D = P->desc[P->rdom[nxt][i]];
+        if (r.cell != kTombstone && D.dl)
+            D.dl[r.cell] = r.dl;
+    }
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -792,7 +1042,7 @@ void unpin_problem(Problem &p) {
 
 size_t Pool::slot_bytes(const Problem &p) {
     size_t N = (size_t)p.g.domain_size, A = (size_t)p.g.active_size;
-    return N * (1 + 4 + 4 + 1 + 4) + A * (4 + 12 + 104 + 8) + p.nuclei_loc.size() * 8 + 64 * 1024;
+    return N * (1 + 4 + 4 + 1 + 4) + A * (4 + 12 + 104 + 8 + 4) + p.nuclei_loc.size() * 8 + 64 * 1024;
 }
 
 Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
@@ -821,6 +1071,15 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
         if (kNeighborZ[l] == -1)
             zminus |= 1u << l;
     }
+    int dir[27], opp[26];
+    for (int q = 0; q < 27; q++)
+        dir[q] = -1;
+    for (int l = 0; l < 26; l++)
+        dir[(kNeighborZ[l] + 1) * 9 + (kNeighborX[l] + 1) * 3 + (kNeighborY[l] + 1)] = l;
+    for (int l = 0; l < 26; l++)
+        opp[l] = dir[(1 - kNeighborZ[l]) * 9 + (1 - kNeighborX[l]) * 3 + (1 - kNeighborY[l])];
+    CUDA_OK(cudaMemcpyToSymbol(c_dir, dir, sizeof(dir)));
+    CUDA_OK(cudaMemcpyToSymbol(c_opp, opp, sizeof(opp)));
     CUDA_OK(cudaMemcpyToSymbol(c_itmask, itmask, sizeof(itmask)));
     CUDA_OK(cudaMemcpyToSymbol(c_zplus, &zplus, sizeof(zplus)));
     CUDA_OK(cudaMemcpyToSymbol(c_zminus, &zminus, sizeof(zminus)));
@@ -838,11 +1097,14 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
     }
     PoolState ps;
     std::memset(&ps, 0, sizeof(ps));
-    CUDA_OK(cudaMalloc(&ps.list[0], capacity_ * sizeof(unsigned long long)));
-    CUDA_OK(cudaMalloc(&ps.list[1], capacity_ * sizeof(unsigned long long)));
-    CUDA_OK(cudaMalloc(&ps.mask, capacity_ * sizeof(unsigned int)));
+    for (int q = 0; q < 2; q++) {
+        CUDA_OK(cudaMalloc(&ps.rec[q], capacity_ * sizeof(ActiveRec)));
+        CUDA_OK(cudaMalloc(&ps.rdom[q], capacity_ * sizeof(unsigned int)));
+    }
+    CUDA_OK(cudaMalloc(&ps.tgt, capacity_ * sizeof(unsigned long long)));
     ps.capacity = capacity_;
-    ps.cur = 1; // k_step_begin flips to 0 on the first cycle
+    ps.cur = 0;
+    ps.pending = 0;
     ps.n_domains = 0;
     ps.desc = ddesc_;
     CUDA_OK(cudaMemcpy(dstate_, &ps, sizeof(ps), cudaMemcpyHostToDevice));
@@ -867,9 +1129,11 @@ Pool::~Pool() {
     if (dstate_) {
         PoolState ps;
         if (cudaMemcpy(&ps, dstate_, sizeof(ps), cudaMemcpyDeviceToHost) == cudaSuccess) {
-            cudaFree(ps.list[0]);
-            cudaFree(ps.list[1]);
-            cudaFree(ps.mask);
+            for (int q = 0; q < 2; q++) {
+                cudaFree(ps.rec[q]);
+                cudaFree(ps.rdom[q]);
+            }
+            cudaFree(ps.tgt);
         }
         cudaFree(dstate_);
     }
@@ -961,6 +1225,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     d.doc = dalloc<float>(3 * A, s.allocs, s.bytes);
     d.cdl = dalloc<float>(26 * A, s.allocs, s.bytes);
     d.claim = dalloc<unsigned long long>(A, s.allocs, s.bytes);
+    d.lmask = dalloc<unsigned int>(A, s.allocs, s.bytes);
     // nuclei in time order; ties keep the reference's order (order does not change results)
     size_t P = p.nuclei_loc.size();
     std::vector<int> order(P);
@@ -981,6 +1246,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     CUDA_OK(cudaMemcpyAsync(d.du, p.du.data(), N * 4, cudaMemcpyHostToDevice, st));
     CUDA_OK(cudaMemsetAsync(d.dl, 0, A * 4, st));
     CUDA_OK(cudaMemsetAsync(d.claim, 0xff, A * 8, st));
+    CUDA_OK(cudaMemsetAsync(d.lmask, 0x80, A * 4, st)); // kMaskFresh in every cell
     if (P) {
         CUDA_OK(cudaMemcpyAsync(dnl, nl.data(), P * 4, cudaMemcpyHostToDevice, st));
         CUDA_OK(cudaMemcpyAsync(dnt, nt.data(), P * 4, cudaMemcpyHostToDevice, st));
@@ -1039,7 +1305,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     int n_domains = std::max(ps.n_domains, slot + 1);
     CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, n_domains), &n_domains, sizeof(int),
                             cudaMemcpyHostToDevice, st));
-    int next_slot = ps.cur ^ 1;
+    int next_slot = ps.pending;
     k_init_active<<<num_sms_ * 4, 256, 0, st>>>(dstate_, slot, next_slot);
     CUDA_OK(cudaGetLastError());
     CUDA_OK(cudaStreamSynchronize(st));
@@ -1079,15 +1345,19 @@ void Pool::launch_step() {
     if (grid_grow_ == 0) {
         // persistent grids: every resident block slot on the device, grid-stride over the list
         int b1 = 0, b2 = 0;
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_grow_claim, kBlock, 0));
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_capture<true>, kBlock, 0));
+        int b3 = 0;
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_grow, kBlock, 0));
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_resolve<true>, kBlock, 0));
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_claim, kBlock, 0));
         grid_grow_ = num_sms_ * std::max(b1, 1);
         grid_capture_ = num_sms_ * std::max(b2, 1);
+        grid_claim_ = num_sms_ * std::max(b3, 1);
     }
     k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
-    k_grow_claim<<<grid_grow_, kBlock, 0, st>>>(dstate_);
-    k_capture<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
-    launches_ += 3;
+    k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+    k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
+    k_resolve<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+    launches_ += 4;
 }
 
 // n cycles in one stream sequence: the begin of cycles 2..n runs in the tail of the previous
@@ -1101,13 +1371,14 @@ void Pool::launch_cycles(int n) {
         return;
     cudaStream_t st = S(stream_);
     k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
-    launches_ += 1 + 2ull * n;
+    launches_ += 1 + 3ull * n;
     for (int q = 0; q < n; q++) {
-        k_grow_claim<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+        k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+        k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
         if (q + 1 < n)
-            k_capture<true><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+            k_resolve<true><<<grid_capture_, kBlock, 0, st>>>(dstate_);
         else
-            k_capture<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+            k_resolve<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
     }
 }
 
@@ -1148,7 +1419,7 @@ void Pool::step(int n) {
     int full = n / graph_steps_, rest = n % graph_steps_;
     for (int q = 0; q < full; q++)
         CUDA_OK(cudaGraphLaunch((cudaGraphExec_t)graph_exec_, st));
-    launches_ += (unsigned long long)full * (1 + 2ull * graph_steps_);
+    launches_ += (unsigned long long)full * (1 + 3ull * graph_steps_);
     launch_cycles(rest);
     CUDA_OK(cudaGetLastError());
 }
@@ -1174,7 +1445,7 @@ unsigned long long Pool::list_count() {
     PoolState ps;
     CUDA_OK(cudaMemcpyAsync(&ps, dstate_, sizeof(ps), cudaMemcpyDeviceToHost, S(stream_)));
     CUDA_OK(cudaStreamSynchronize(S(stream_)));
-    return ps.cnt[ps.cur ^ 1];
+    return ps.cnt[ps.pending];
 }
 
 PoolStats Pool::stats() {
@@ -1191,8 +1462,10 @@ PoolStats Pool::stats() {
         r.captured += ps.stat[q][kStatCaptured];
         r.nucleated += ps.stat[q][kStatNucleated];
         r.claims += ps.stat[q][kStatClaims];
-        r.liquid_nb += ps.stat[q][kStatLiquidNb];
+        r.row_reads += ps.stat[q][kStatRowReads];
         r.kept += ps.stat[q][kStatKept];
+        r.fresh += ps.stat[q][kStatFresh];
+        r.rechecks += ps.stat[q][kStatRechecks];
     }
     return r;
 }
@@ -1221,9 +1494,10 @@ KernelTimes Pool::profile_cycles(int n) {
         CUDA_OK(cudaEventRecord(ev[0], st));
         k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[1], st));
-        k_grow_claim<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+        k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+        k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[2], st));
-        k_capture<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+        k_resolve<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[3], st));
         CUDA_OK(cudaEventSynchronize(ev[3]));
         float a, b, c;
@@ -1238,7 +1512,7 @@ KernelTimes Pool::profile_cycles(int n) {
         CUDA_OK(cudaEventDestroy(e));
     kt.cycles = n;
     cycles_launched_ += n;
-    launches_ += 3ull * n;
+    launches_ += 4ull * n;
     return kt;
 }
 
@@ -1292,8 +1566,15 @@ void Pool::copy_out_raw(int slot, int32_t *grain_id, int8_t *cell_type) {
     CUDA_OK(cudaStreamSynchronize(st));
 }
 
-void Pool::copy_octahedra(int slot, float *dl, float *doc, float *cdl) {
+void Pool::flush_records() {
     CUDA_OK(cudaSetDevice(device_));
+    k_flush_records<<<num_sms_ * 2, 256, 0, S(stream_)>>>(dstate_);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaStreamSynchronize(S(stream_)));
+}
+
+void Pool::copy_octahedra(int slot, float *dl, float *doc, float *cdl) {
+    flush_records();
     const DomainDesc &d = host_desc_.at(slot);
     size_t A = slots_.at(slot).problem->g.active_size;
     cudaStream_t st = S(stream_);

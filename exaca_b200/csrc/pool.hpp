@@ -6,6 +6,7 @@
 // by one CA cycle. The step loop is replayed as a captured CUDA graph.
 #pragma once
 
+#include <cstddef>
 #include <cstdint>
 #include <map>
 #include <memory>
@@ -17,19 +18,35 @@
 namespace exaca {
 
 constexpr int kMaxJumps = 32;
+constexpr unsigned int kTombstone = 0xffffffffu;
 constexpr int kLiquidShards = 16;
 constexpr int kStatShards = 32;
 // pool statistics, summed over shards
 enum {
-    kStatListed = 0,    // active-list entries visited
-    kStatGrown = 1,     // entries grown (eligible)
+    kStatListed = 0,    // active-cell records visited
+    kStatGrown = 1,     // records grown (eligible)
     kStatCaptured = 2,  // captures
     kStatNucleated = 3, // nucleation events
     kStatClaims = 4,    // atomicMin claims issued
-    kStatLiquidNb = 5,  // liquid neighbours seen by grown entries
-    kStatKept = 6,      // entries carried into the next list
-    kNumStats = 8
+    kStatRowReads = 5,  // critical-diagonal-length rows read (diagonal reached the cached minimum)
+    kStatKept = 6,      // records carried into the next list
+    kStatFresh = 7,     // liquid-neighbour masks built from the 26 neighbour types
+    kStatRechecks = 8,  // solidification re-checks around claimed cells
+    kStatDropped = 9,   // records dropped by the growth pass
+    kStatFlagged = 10,  // records the growth pass handed to the claim pass
+    kNumStats = 11
 };
+
+// One active cell in the compacted list: the state the per-cycle growth pass needs, so that pass
+// streams 16-byte records instead of gathering per-cell arrays.
+struct alignas(16) ActiveRec {
+    float dl;          // DiagonalLength (dl and cdl_min form one aligned 8-byte pair)
+    float cdl_min;     // lower bound of the critical lengths of the cell's liquid neighbours
+    unsigned int cell; // index in the domain; kTombstone for a dropped record
+    int cts;           // CritTimeStep
+};
+static_assert(sizeof(ActiveRec) == 16, "ActiveRec is one 16-byte vector");
+static_assert(offsetof(ActiveRec, dl) % 8 == 0, "dl/cdl_min are stored as one float2");
 
 // Device-resident descriptor of one domain. Static fields are written at admission; dynamic
 // fields are advanced by the step kernels and read back by the host.
@@ -44,6 +61,7 @@ struct DomainDesc {
     float *doc;               // 3 per active-window cell
     float *cdl;               // 26 per active-window cell
     unsigned long long *claim; // per active-window cell: (~epoch << 32) | capturer index
+    unsigned int *lmask;      // per active-window cell: liquid-neighbour directions (kMaskFresh: not known yet)
     const double *growth;     // growth increment by number of undercooling updates
     const float *guv;         // 9 per orientation
     const float *cdl_table;   // 26 per orientation
@@ -72,28 +90,34 @@ struct DomainDesc {
 
 // Pool-level device state.
 struct PoolState {
-    unsigned long long *list[2]; // entries: (domain << 32) | cell
-    unsigned int *mask;          // per entry of the current list
+    ActiveRec *rec[2];           // active-cell records of the current / next cycle
+    unsigned int *rdom[2];       // domain of each record
+    unsigned long long *tgt;     // cells claimed this cycle: (domain << 32) | cell
     unsigned long long cnt[2];
+    unsigned long long tcnt;
     unsigned long long capacity;
-    int cur;
+    unsigned long long tombs; // dropped records still in list `cur` (in-place cycles)
+    int cur;                  // list read by this cycle's growth pass
+    int pending;              // list the next cycle reads (cur, or cur ^ 1 when this cycle compacts)
+    int compact;              // 1: this cycle's growth pass writes the survivors to list cur ^ 1
     int error;
     int n_domains;
     int pad;
     DomainDesc *desc;
     unsigned long long stat[kStatShards][kNumStats];
-    unsigned int blocks_done; // last-block detection of the capture kernel
+    unsigned int blocks_done;      // last-block detection of the resolve kernel
+    unsigned long long work[2];    // dynamic chunk counters of the claim and resolve passes
 };
 
 struct PoolStats {
     unsigned long long cycles; // CA cycles launched
     unsigned long long launches; // kernels launched by step()
-    unsigned long long listed, grown, captured, nucleated, claims, liquid_nb, kept;
+    unsigned long long listed, grown, captured, nucleated, claims, row_reads, kept, fresh, rechecks;
 };
 
 // Per-kernel CUDA-event times of a profiled stretch of cycles.
 struct KernelTimes {
-    double begin_ms = 0, grow_ms = 0, capture_ms = 0;
+    double begin_ms = 0, grow_ms = 0, capture_ms = 0; // capture_ms: the claimed-cell pass
     int cycles = 0;
 };
 
@@ -142,6 +166,8 @@ class Pool {
     void copy_out(int slot, int32_t *grain_id, int32_t *cell_type);
     void copy_out_raw(int slot, int32_t *grain_id, int8_t *cell_type);
     void copy_octahedra(int slot, float *dl, float *doc, float *cdl);
+    // writes the diagonal lengths held in the active records back to the per-cell array
+    void flush_records();
     // Reference-equivalent run of one slot to completion with the reference's 1000-cycle census,
     // stdout progress lines and type-S cycle jumps (src/runCA.cpp:290-342).
     int run_plain(int slot, std::string &log, double *nucl_s, double *capture_s);
@@ -183,7 +209,7 @@ class Pool {
     std::map<std::string, DeviceTables> tables_;
     int num_sms_ = 148;
     unsigned long long cycles_launched_ = 0;
-    int grid_grow_ = 0, grid_capture_ = 0;
+    int grid_grow_ = 0, grid_capture_ = 0, grid_claim_ = 0;
     unsigned long long launches_ = 0;
     double last_run_ms_ = 0;
     void *census_buf_ = nullptr;

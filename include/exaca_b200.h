@@ -72,8 +72,10 @@ typedef struct {
     uint64_t captured;  /* liquid cells captured */
     uint64_t nucleated; /* nucleation events */
     uint64_t claims;    /* capture claims issued */
-    uint64_t liquid_nb; /* liquid neighbours examined by grown cells */
+    uint64_t row_reads; /* critical-diagonal-length rows read (diagonal reached the cached minimum) */
     uint64_t kept;      /* list entries carried to the next cycle */
+    uint64_t fresh;     /* liquid-neighbour masks built from the 26 neighbour types */
+    uint64_t rechecks;  /* solidification re-checks next to claimed cells */
 } exaca_pool_stats_t;
 
 /* The reference's every-1000-cycle census (src/CAupdate.cpp:738-808). */
@@ -118,7 +120,7 @@ int exaca_pool_admit(exaca_pool *pool, const exaca_problem *p, int device_check,
 int exaca_pool_step(exaca_pool *pool, int n_cycles);
 /* Waits for the device and reads one slot's state. */
 int exaca_pool_status(exaca_pool *pool, int slot, exaca_domain_status *st);
-/* Waits for the device and reads the pool's work counters. */
+/* Waits for the device and reads the pool's work counters (summed over all domains). */
 int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st);
 /* IntermediateOutputAndCheck's census (src/CAupdate.hpp:30-33) for one slot. */
 int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c);
