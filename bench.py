@@ -37,9 +37,24 @@ UNIT = "cell-updates/s"
 WORKLOAD = dict(G=1e6, R=1e6, n_ratio=25, nucleation_density=100.0, dTN=3.0, dTsigma=0.5, fract_surface_active=0.02)
 REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
 
-# algorithmic bytes per unit of work of the two step kernels ("Roofline")
-GROW_BYTES = dict(listed=12, grown=142, claims=8)
-CAPTURE_BYTES = dict(listed=12, kept=8, liquid_nb=8, captured=185)
+# Algorithmic bytes of each step kernel per unit of work (the bytes the kernel must read or write,
+# each counted once per use, no cache reuse credited):
+#   k_grow:       record 16 + domain 4 + liquid mask 4 + growth-table entry 8 per listed record;
+#                 diagonal/min-length write 8 per grown record; tombstone 16 + DiagonalLength 4
+#                 per dropped record; queue entry 4 per flagged record
+#   k_claim:      queue 4 + record 16 + mask 4 + critical-length row 104 + min write 4 per flagged
+#                 record; 26 neighbour types + mask write 4 per fresh mask; 8 per claim; 8 per
+#                 claimed cell listed
+#   k_capture:    per capture: claim 8, target 8, GrainID 4+4, centres 12+12, orientation 36,
+#                 DiagonalLength 4, 26 critical lengths 104, mask 4, record 16+4, CellType 1, CritTimeStep 4
+#   k_neighbours: 9 per neighbour item (26 per capture); per re-check: mask clear 4 + mask 4 +
+#                 CritTimeStep 4 + 26 claims 208
+KERNEL_BYTES = {
+    "k_grow": dict(listed=32, grown=8, dropped=20, flagged=4),
+    "k_claim": dict(flagged=132, fresh=30, claims=8, captured=8),
+    "k_capture": dict(captured=221),
+    "k_neighbours": dict(captured=9 * 26, rechecks=220),
+}
 
 
 def input_file_text(n):
@@ -274,9 +289,10 @@ def b200_arm(args, rank, world, local):
     pb = pool.stats()
     pool.retire(slot)
     d = {k: pb[k] - pa[k] for k in pb}
-    grow_bytes = sum(GROW_BYTES[k] * d[k] for k in GROW_BYTES)
-    cap_bytes = sum(CAPTURE_BYTES[k] * d[k] for k in CAPTURE_BYTES)
-    kernels = {"k_grow_claim": (kt["grow_ms"], grow_bytes), "k_capture": (kt["capture_ms"], cap_bytes)}
+    kernels = {}
+    for k, model in KERNEL_BYTES.items():
+        b = sum(per * d[unit] for unit, per in model.items())
+        kernels[k] = (kt[k], b)
     dom = max(kernels, key=lambda k: kernels[k][0])
     dom_ms, dom_bytes = kernels[dom]
     peak, peak_kind = peaks()
@@ -310,7 +326,9 @@ def b200_arm(args, rank, world, local):
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": per_launch_bytes,
                          "sample": f"cycles {args.profile_at + 1}-{args.profile_at + args.profile_cycles}",
-                         "kernel_ms": {k: v[0] / max(1, args.profile_cycles) for k, v in kernels.items()},
+                         "kernel_ms_per_launch": {k: v[0] / max(1, args.profile_cycles) for k, v in kernels.items()},
+                         "kernel_gbs": {k: v[1] / (v[0] / 1e3) / 1e9 for k, v in kernels.items() if v[0] > 0},
+                         "begin_ms_per_launch": kt["k_step_begin"] / max(1, args.profile_cycles),
                          "effective_dense_frac": value / world * eff_bytes_per_update / 1e9 / peak},
         }
         if world == 1 and not args.no_cpu_baseline:

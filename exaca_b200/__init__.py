@@ -73,8 +73,8 @@ class DomainStatus(ctypes.Structure):
 
 class PoolStatsT(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in
-                ("cycles", "launches", "listed", "grown", "captured", "nucleated", "claims", "row_reads", "kept",
-                 "fresh", "rechecks")]
+                ("cycles", "launches", "listed", "grown", "captured", "nucleated", "claims", "row_reads", "dropped",
+                 "fresh", "rechecks", "flagged")]
 
 
 class CensusT(ctypes.Structure):
@@ -267,9 +267,9 @@ class Pool:
 
     def profile_cycles(self, n_cycles: int) -> dict:
         """Runs n cycles kernel by kernel with CUDA events around each launch; summed ms per kernel."""
-        t = (ctypes.c_double * 3)()
+        t = (ctypes.c_double * 5)()
         _check(load_library().exaca_pool_profile_cycles(self._h, n_cycles, t))
-        return {"begin_ms": t[0], "grow_ms": t[1], "capture_ms": t[2]}
+        return {"k_step_begin": t[0], "k_grow": t[1], "k_claim": t[2], "k_capture": t[3], "k_neighbours": t[4]}
 
     def retire(self, slot: int) -> None:
         _check(load_library().exaca_pool_retire(self._h, slot))

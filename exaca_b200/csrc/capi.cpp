@@ -238,9 +238,10 @@ int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st) {
         st->nucleated = s.nucleated;
         st->claims = s.claims;
         st->row_reads = s.row_reads;
-        st->kept = s.kept;
+        st->dropped = s.dropped;
         st->fresh = s.fresh;
         st->rechecks = s.rechecks;
+        st->flagged = s.flagged;
     });
 }
 
@@ -253,7 +254,9 @@ int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms)
         exaca::KernelTimes t = pool->pool->profile_cycles(n_cycles);
         kernel_ms[0] = t.begin_ms;
         kernel_ms[1] = t.grow_ms;
-        kernel_ms[2] = t.capture_ms;
+        kernel_ms[2] = t.claim_ms;
+        kernel_ms[3] = t.capture_ms;
+        kernel_ms[4] = t.neighbours_ms;
     });
 }
 

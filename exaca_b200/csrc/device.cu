@@ -2,7 +2,7 @@
 //
 // One CA cycle (src/runCA.cpp:290-341; src/CAupdate.cpp:67-728) is three kernels over a pool of
 // domains:
-//   begin (k_step_begin, or the tail of the previous k_resolve): per domain, the device-side
+//   begin (k_step_begin, or the tail of the previous k_neighbours): per domain, the device-side
 //          termination check, cycle/epoch advance and nucleation of the sites whose time has come
 //          (nuclei are pre-sorted by time, one cursor each).
 //   k_grow: streams the 16-byte records of the active cells (shared compacted list): diagonal
@@ -11,7 +11,7 @@
 //          the octahedron reaches. Liquid neighbours come from a per-cell mask kept up to date by
 //          captures and nucleations; the 26 critical lengths are read only when the diagonal has
 //          reached the cached minimum over the liquid neighbours.
-//   k_resolve: one thread per claimed cell: capture by the lowest-index claimant (new decentred
+//   k_capture / k_neighbours: per claimed cell: capture by the lowest-index claimant (new decentred
 //          octahedron, 26 critical lengths), mask updates of its active neighbours, and for those
 //          the solidification re-check.
 // The claim rule reproduces the Kokkos-Serial loop order exactly: serial visits active cells in
@@ -58,6 +58,7 @@ __constant__ int c_opp[26];
 
 constexpr unsigned int kMaskFresh = 1u << 31; // liquid-neighbour mask not built yet
 constexpr unsigned int kMaskDead = 1u << 30;  // solidified by a re-check: leaves the list next cycle
+constexpr unsigned int kMaskKeep = 1u << 29;  // this cycle, a neighbour was captured by an index >= this cell's
 constexpr unsigned int kDirBits = (1u << 26) - 1;
 constexpr int kErrGrowthTable = 1;
 constexpr int kErrListOverflow = 2;
@@ -81,10 +82,11 @@ __device__ __forceinline__ long long executed_upto(const DomainDesc &D, long lon
     return e;
 }
 
-// Block-aggregated reservation of `n` slots per thread in list `slot`: one atomicAdd per block.
-// Must be called by every thread of the block. Returns this thread's first slot, or ULLONG_MAX on
+// Block-aggregated reservation of `n` slots per thread on `counter`: one atomicAdd per block. Must
+// be called by every thread of the block. Returns this thread's first slot, or ULLONG_MAX on
 // overflow (the pool error flag is set).
-__device__ __forceinline__ unsigned long long block_reserve(PoolState *P, int slot, unsigned int n) {
+__device__ __forceinline__ unsigned long long block_reserve_on(unsigned long long *counter, unsigned long long cap,
+                                                              int *error, unsigned int n) {
     __shared__ unsigned int s_warp[kBlock / 32];
     __shared__ unsigned long long s_base;
     __shared__ int s_ok;
@@ -112,10 +114,10 @@ __device__ __forceinline__ unsigned long long block_reserve(PoolState *P, int sl
             s_warp[lane] = inc2 - v;
         unsigned int total = __shfl_sync(0xffffffffu, inc2, kBlock / 32 - 1);
         if (lane == 0) {
-            unsigned long long b = total ? atomicAdd(&P->cnt[slot], (unsigned long long)total) : 0ull;
-            s_ok = (b + total <= P->capacity);
+            unsigned long long b = total ? atomicAdd(counter, (unsigned long long)total) : 0ull;
+            s_ok = (b + total <= cap);
             if (!s_ok)
-                atomicOr(&P->error, kErrListOverflow);
+                atomicOr(error, kErrListOverflow);
             s_base = b;
         }
     }
@@ -123,6 +125,10 @@ __device__ __forceinline__ unsigned long long block_reserve(PoolState *P, int sl
     unsigned long long r = s_ok ? s_base + s_warp[warp] + (incl - n) : ULLONG_MAX;
     __syncthreads(); // s_warp / s_base are reused by the next call
     return r;
+}
+
+__device__ __forceinline__ unsigned long long block_reserve(PoolState *P, int slot, unsigned int n) {
+    return block_reserve_on(&P->cnt[slot], P->capacity, &P->error, n);
 }
 
 // Warp-aggregated reservation (any subset of lanes may call, all with the same counter).
@@ -230,23 +236,21 @@ __device__ __forceinline__ long long domain_liquid(const DomainDesc &D) {
 // ---------------------------------------------------------------------------------------------
 // Capture of liquid cell t by active cell c through neighbour direction l
 // (src/CAupdate.cpp:353-563, 713-717).
-__device__ void capture_cell(const DomainDesc &D, long long c, long long t, int l) {
-    int plane = D.mx * D.my;
-    int rz = (int)(c / plane);
-    int rem = (int)(c - (long long)rz * plane);
-    int rx = rem / D.my;
-    int ry = rem - rx * D.my;
-    int GlobalX = rx + D.xoff, GlobalY = ry + D.yoff, GlobalZ = rz;
-    int h = D.gid[c];
+__device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int t, int l) {
+    // all loads first: capturer state, then its orientation
+    const int h = D.gid[c];
+    const float docx = D.doc[3ull * c + 0], docy = D.doc[3ull * c + 1], docz = D.doc[3ull * c + 2];
+    int rx, ry, rz;
+    cell_coords(D, c, rx, ry, rz);
+    const int GlobalX = rx + D.xoff, GlobalY = ry + D.yoff, GlobalZ = rz;
     int ori = (abs(h) - 1) % 10000;
     if (ori < 0)
         ori += 10000;
     const float *g = D.guv + 9 * ori;
     const float g0 = g[0], g1 = g[1], g2 = g[2], g3 = g[3], g4 = g[4], g5 = g[5], g6 = g[6], g7 = g[7], g8 = g[8];
-    D.gid[t] = h;
-    double cxold = D.doc[3 * c + 0];
-    double cyold = D.doc[3 * c + 1];
-    double czold = D.doc[3 * c + 2];
+    const double cxold = docx;
+    const double cyold = docy;
+    const double czold = docz;
     double xp = GlobalX + c_nx[l] + 0.5;
     double yp = GlobalY + c_ny[l] + 0.5;
     double zp = GlobalZ + c_nz[l] + 0.5;
@@ -310,6 +314,7 @@ __device__ void capture_cell(const DomainDesc &D, long long c, long long t, int 
     double L12 = 0.5 * (dmin(I1, sqrt3) + dmin(I2, sqrt3));
     double L13 = 0.5 * (dmin(J1, sqrt3) + dmin(J2, sqrt3));
     double NewODiagL = sqrt(2.0) * dmax(L12, L13);
+    D.gid[t] = h;
     D.dl[t] = (float)NewODiagL;
     double cd0 = xc - cxold, cd1 = yc - cyold, cd2 = zc - czold;
     double nd = sqrt(cd0 * cd0 + cd1 * cd1 + cd2 * cd2);
@@ -347,36 +352,7 @@ __device__ void capture_cell(const DomainDesc &D, long long c, long long t, int 
         double m = dmax(dmax(fabs(q0), fabs(q1)), dmax(fabs(q2), fabs(q3)));
         out[n] = (float)m;
     }
-}
-
-// Does active cell a still see a liquid neighbour at the end of this cycle's serial order? Its
-// neighbours that were liquid at the start of the cycle are the claimed ones plus the unclaimed
-// bits of its mask (only captures clear mask bits, and every capture was claimed). Captured by a
-// lower index = seen as active; otherwise seen as liquid (src/CAupdate.cpp:333-334, 722-725).
-// All 26 claim words are loaded before any is examined.
-__device__ bool still_sees_liquid(const DomainDesc &D, unsigned int a) {
-    int rx, ry, rz;
-    cell_coords(D, a, rx, ry, rz);
-    const unsigned int valid = neighbour_mask(D, rx, ry, rz);
-    const unsigned int m = __ldcg(D.lmask + a);
-    const unsigned int want = 0xffffffffu - D.epoch;
-    const int plane = D.mx * D.my, my = D.my;
-    const unsigned long long *claim = D.claim + a;
-    unsigned long long k[26];
-#pragma unroll
-    for (int l = 0; l < 26; l++)
-        k[l] = (valid & (1u << l)) ? __ldcg(claim + nb_offset(l, plane, my)) : 0ull;
-    bool sees = false;
-#pragma unroll
-    for (int l = 0; l < 26; l++) {
-        if (valid & (1u << l)) {
-            if ((unsigned int)(k[l] >> 32) == want)
-                sees |= (unsigned int)k[l] >= a;
-            else
-                sees |= (m >> l) & 1u;
-        }
-    }
-    return sees;
+    return (float)NewODiagL;
 }
 
 // A nucleation site stopped being liquid: its active neighbours drop it from their masks.
@@ -416,8 +392,7 @@ __device__ void begin_cycle(PoolState *P) {
         if (compact)
             P->cnt[cur ^ 1] = 0;
         P->tcnt = 0;
-        P->work[0] = 0;
-        P->work[1] = 0;
+        P->qcnt = 0;
         s_cur = cur;
     }
     __syncthreads();
@@ -549,6 +524,11 @@ __device__ __forceinline__ int grow_record(DomainDesc &D, ActiveRec &r, unsigned
 __device__ __forceinline__ void load_growth(const DomainDesc &D, const ActiveRec &r, unsigned int &m, double &inc,
                                             bool &ok) {
     m = D.lmask[r.cell];
+    if (m & kMaskKeep) {
+        // the neighbour verdict of the previous cycle does not carry over
+        m &= ~kMaskKeep;
+        D.lmask[r.cell] = m;
+    }
     // undercooling after the executed updates since the liquidus (src/CAupdate.cpp:236-237)
     long long nu = executed_upto(D, D.cycle) - executed_upto(D, r.cts);
     if (D.zero_du && D.du[r.cell] == 0.0f)
@@ -567,8 +547,9 @@ __global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
     if (!P->compact) {
         // records are updated in place; dropped ones become tombstones
         const unsigned long long step = (unsigned long long)gridDim.x * kBlock * kBatch;
-        for (unsigned long long base = (unsigned long long)blockIdx.x * kBlock * kBatch + threadIdx.x; base < n;
-             base += step) {
+        // block-uniform loop: block_reserve_on is reached by every thread
+        for (unsigned long long b0 = (unsigned long long)blockIdx.x * kBlock * kBatch; b0 < n; b0 += step) {
+            const unsigned long long base = b0 + threadIdx.x;
             ActiveRec r[kBatch];
             unsigned int dom[kBatch], m[kBatch];
             double inc[kBatch];
@@ -591,6 +572,7 @@ __global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
                 if (r[q].cell != kTombstone)
                     load_growth(desc[dom[q]], r[q], m[q], inc[q], ok[q]);
             }
+            unsigned int flagged = 0;
 #pragma unroll
             for (int q = 0; q < kBatch; q++) {
                 if (r[q].cell == kTombstone)
@@ -606,7 +588,17 @@ __global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
                 }
                 else if (a == 2) {
                     *reinterpret_cast<float2 *>(&in[i].dl) = make_float2(r[q].dl, r[q].cdl_min);
+                    if (__float_as_uint(r[q].cdl_min) == kNeedsClaim)
+                        flagged |= 1u << q;
                 }
+            }
+            const unsigned long long qpos = block_reserve_on(&P->qcnt, P->capacity, &P->error, __popc(flagged));
+            if (qpos != ULLONG_MAX) {
+                unsigned long long k = qpos;
+#pragma unroll
+                for (int q = 0; q < kBatch; q++)
+                    if (flagged & (1u << q))
+                        P->queue[k++] = (unsigned int)(base + (unsigned long long)q * kBlock);
             }
         }
     }
@@ -634,10 +626,14 @@ __global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
                 }
             }
             const unsigned long long pos = block_reserve(P, nxt, keep ? 1u : 0u);
+            const bool flag = keep && pos != ULLONG_MAX && __float_as_uint(r.cdl_min) == kNeedsClaim;
             if (keep && pos != ULLONG_MAX) {
                 out[pos] = r;
                 out_dom[pos] = dom;
             }
+            const unsigned long long qpos = block_reserve_on(&P->qcnt, P->capacity, &P->error, flag ? 1u : 0u);
+            if (flag && qpos != ULLONG_MAX)
+                P->queue[qpos] = (unsigned int)pos;
         }
     }
     block_stats(P, st.listed, st.grown, kStatListed, kStatGrown);
@@ -656,30 +652,16 @@ __global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
     }
 }
 
-// Next chunk of kBlock work items for this block, handed out by an atomic counter.
-__device__ __forceinline__ unsigned long long next_chunk(unsigned long long *counter) {
-    __shared__ unsigned long long s_chunk;
-    __syncthreads();
-    if (threadIdx.x == 0)
-        s_chunk = atomicAdd(counter, 1ull);
-    __syncthreads();
-    return s_chunk;
-}
-
 __global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
     const int lst = P->pending; // the list the growth pass just wrote
-    const unsigned long long n = P->cnt[lst];
+    const unsigned long long nq = P->qcnt;
     ActiveRec *recs = P->rec[lst];
     const unsigned int *rdom = P->rdom[lst];
     DomainDesc *desc = P->desc;
     unsigned long long st_claims = 0, st_rows = 0, st_fresh = 0, st_dropped = 0;
-    for (;;) {
-        const unsigned long long chunk = next_chunk(&P->work[0]);
-        const unsigned long long i = chunk * kBlock + threadIdx.x;
-        if (chunk * kBlock >= n)
-            break;
-        if (i >= n)
-            continue;
+    for (unsigned long long qi = (unsigned long long)blockIdx.x * kBlock + threadIdx.x; qi < nq;
+         qi += (unsigned long long)gridDim.x * kBlock) {
+        const unsigned long long i = P->queue[qi];
         const ActiveRec rec = recs[i];
         if (rec.cell == kTombstone || __float_as_uint(rec.cdl_min) != kNeedsClaim)
             continue;
@@ -738,7 +720,7 @@ __global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
         recs[i].cdl_min = nm;
         if (reach) {
             // claims (src/CAupdate.cpp:336-352): lowest index wins; the first claimant of a cell in
-            // this cycle lists it for k_resolve
+            // this cycle lists it for k_capture / k_neighbours
             const unsigned long long key = ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
             const unsigned int want = 0xffffffffu - D.epoch;
             unsigned int first = 0;
@@ -765,82 +747,93 @@ __global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
         atomicAdd(&P->tombs, st_dropped);
 }
 
-// k_resolve: every cell claimed this cycle is captured by its lowest-index claimant
-// (src/CAupdate.cpp:336-563, 713-717), its active neighbours drop it from their liquid masks, and
-// those grown this cycle re-check whether they still see a liquid neighbour
-// (src/CAupdate.cpp:722-725). Work items (captures first, then 26 neighbour updates per claimed
-// cell) are handed out in chunks. With kTail the last block to finish starts the next cycle.
-template <bool kTail> __global__ void __launch_bounds__(kBlock) k_resolve(PoolState *P) {
+// Every cell claimed this cycle is captured by its lowest-index claimant (src/CAupdate.cpp:336-563,
+// 713-717). Two independent passes over the claimed cells:
+//   k_capture     one thread per claimed cell: the new octahedron, 26 critical lengths, GrainID,
+//                 and its record in the next cycle's list.
+//   k_neighbours  26 threads per claimed cell: each active neighbour drops the cell from its liquid
+//                 mask, and a neighbour grown this cycle re-checks whether it still sees a liquid
+//                 cell (src/CAupdate.cpp:722-725). With kTail the last block to finish starts the
+//                 next cycle.
+// Neither pass reads what the other writes: the re-check uses the claims and the unclaimed mask
+// bits only, and a cell being captured still has its initial (not yet built) mask.
+__global__ void __launch_bounds__(kBlock) k_capture(PoolState *P) {
     const int app = P->pending; // list of the next cycle
     const unsigned long long T = P->tcnt;
-    const unsigned long long n = T * 27ull;
     DomainDesc *desc = P->desc;
-    unsigned long long st_cap = 0, st_rc = 0;
-    for (;;) {
-        const unsigned long long chunk = next_chunk(&P->work[1]);
-        if (chunk * kBlock >= n)
-            break;
-        const unsigned long long j = chunk * kBlock + threadIdx.x;
-        if (j >= n)
-            continue;
-        if (j < T) {
-            const unsigned long long e = P->tgt[j];
-            const unsigned int dom = (unsigned int)(e >> 32);
-            const unsigned int t = (unsigned int)e;
-            DomainDesc &D = desc[dom];
-            const unsigned int w = (unsigned int)__ldcg(D.claim + t);
-            int wx, wy, wz, tx, ty, tz;
-            cell_coords(D, w, wx, wy, wz);
-            cell_coords(D, t, tx, ty, tz);
-            const int l = c_dir[(tz - wz + 1) * 9 + (tx - wx + 1) * 3 + (ty - wy + 1)];
-            capture_cell(D, w, t, l);
-            D.lmask[t] = kMaskFresh;
-            unsigned long long pos = warp_reserve(&P->cnt[app], P->capacity, &P->error);
-            if (pos != ULLONG_MAX) {
-                ActiveRec r;
-                r.cell = t;
-                r.dl = __ldcg(D.dl + t);
-                r.cdl_min = 0.0f;
-                r.cts = __ldg(D.cts + t);
-                P->rec[app][pos] = r;
-                P->rdom[app][pos] = dom;
-            }
-            // the captured cell becomes active only after its octahedron data is written
-            D.ctype[t] = kActive;
-            atomicAdd((unsigned long long *)&D.liquid_shard[blockIdx.x & (kLiquidShards - 1)],
-                      (unsigned long long)(-1ll));
-            st_cap++;
+    unsigned long long st_cap = 0;
+    for (unsigned long long j = (unsigned long long)blockIdx.x * kBlock + threadIdx.x; j < T;
+         j += (unsigned long long)gridDim.x * kBlock) {
+        const unsigned long long e = P->tgt[j];
+        const unsigned int dom = (unsigned int)(e >> 32);
+        const unsigned int t = (unsigned int)e;
+        DomainDesc &D = desc[dom];
+        const unsigned int w = (unsigned int)__ldcg(D.claim + t);
+        const int cts_t = __ldg(D.cts + t);
+        int wx, wy, wz, tx, ty, tz;
+        cell_coords(D, w, wx, wy, wz);
+        cell_coords(D, t, tx, ty, tz);
+        const int l = c_dir[(tz - wz + 1) * 9 + (tx - wx + 1) * 3 + (ty - wy + 1)];
+        const float new_dl = capture_cell(D, w, t, l);
+        D.lmask[t] = kMaskFresh;
+        unsigned long long pos = warp_reserve(&P->cnt[app], P->capacity, &P->error);
+        if (pos != ULLONG_MAX) {
+            ActiveRec r;
+            r.cell = t;
+            r.dl = new_dl;
+            r.cdl_min = 0.0f;
+            r.cts = cts_t;
+            P->rec[app][pos] = r;
+            P->rdom[app][pos] = dom;
         }
-        else {
-            // neighbour a of a claimed cell t: drop t from a's liquid mask; a cell grown this
-            // cycle re-checks whether it still sees a liquid neighbour
-            const unsigned long long q = (j - T) / 26ull;
-            const int l = (int)((j - T) - q * 26ull);
-            const unsigned long long e = P->tgt[q];
-            const unsigned int dom = (unsigned int)(e >> 32);
-            const unsigned int t = (unsigned int)e;
-            DomainDesc &D = desc[dom];
-            int tx, ty, tz;
-            cell_coords(D, t, tx, ty, tz);
-            if (!(neighbour_mask(D, tx, ty, tz) & (1u << l)))
-                continue;
-            const unsigned int a = (unsigned int)((long long)t + nb_offset(l, D.mx * D.my, D.my));
-            if (__ldcg(D.ctype + a) != kActive)
-                continue;
-            // the mask bits of claimed cells do not matter to the re-check, so the clear need not
-            // complete first
-            atomicAnd(D.lmask + a, ~(1u << c_opp[l]));
-            const unsigned int m = __ldcg(D.lmask + a);
-            if (!(m & (kMaskFresh | kMaskDead)) && D.cycle > __ldg(D.cts + a)) {
-                st_rc++;
-                if (!still_sees_liquid(D, a)) {
-                    D.ctype[a] = kSolid;
-                    atomicOr(D.lmask + a, kMaskDead);
-                }
-            }
+        // the captured cell becomes active only after its octahedron data is written
+        D.ctype[t] = kActive;
+        atomicAdd((unsigned long long *)&D.liquid_shard[blockIdx.x & (kLiquidShards - 1)], (unsigned long long)(-1ll));
+        st_cap++;
+    }
+    block_stats(P, st_cap, 0, kStatCaptured, kStatCaptured);
+}
+
+template <bool kTail> __global__ void __launch_bounds__(kBlock) k_neighbours(PoolState *P) {
+    const unsigned long long n = P->tcnt * 26ull;
+    DomainDesc *desc = P->desc;
+    unsigned long long st_rc = 0;
+    for (unsigned long long j = (unsigned long long)blockIdx.x * kBlock + threadIdx.x; j < n;
+         j += (unsigned long long)gridDim.x * kBlock) {
+        const unsigned long long q = j / 26ull;
+        const int l = (int)(j - q * 26ull);
+        const unsigned long long e = P->tgt[q];
+        const unsigned int dom = (unsigned int)(e >> 32);
+        const unsigned int t = (unsigned int)e;
+        DomainDesc &D = desc[dom];
+        int tx, ty, tz;
+        cell_coords(D, t, tx, ty, tz);
+        if (!(neighbour_mask(D, tx, ty, tz) & (1u << l)))
+            continue;
+        const unsigned int a = (unsigned int)((long long)t + nb_offset(l, D.mx * D.my, D.my));
+        const unsigned int w = (unsigned int)__ldcg(D.claim + t);
+        if (__ldcg(D.ctype + a) != kActive)
+            continue;
+        // Serial order (src/CAupdate.cpp:333-334, 722-725): active cell a saw the captured cell t
+        // as liquid iff t's capturer w does not precede a. a keeps a liquid neighbour iff it has an
+        // unclaimed one (a set mask bit that nobody clears) or a claimed one with w >= a. Every
+        // claimed liquid neighbour clears its own bit exactly once, so the update that clears the
+        // last direction bit sees the final verdict: KEEP is always set before the clear of the
+        // same update, and an update's two atomics reach the word in program order.
+        if (w >= a)
+            atomicOr(D.lmask + a, kMaskKeep);
+        const unsigned int bit = 1u << c_opp[l];
+        const unsigned int old = atomicAnd(D.lmask + a, ~bit);
+        if ((old & (kMaskFresh | kMaskDead)) || (old & kDirBits) != bit || (old & kMaskKeep))
+            continue;
+        // a lost its last liquid neighbour; it solidifies if it was grown this cycle
+        if (D.cycle > __ldg(D.cts + a)) {
+            st_rc++;
+            D.ctype[a] = kSolid;
+            atomicOr(D.lmask + a, kMaskDead);
         }
     }
-    block_stats(P, st_cap, st_rc, kStatCaptured, kStatRechecks);
+    block_stats(P, st_rc, 0, kStatRechecks, kStatRechecks);
     if (kTail) {
         __shared__ int s_last;
         __threadfence(); // this block's writes are visible device-wide before it is counted
@@ -1102,6 +1095,7 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
         CUDA_OK(cudaMalloc(&ps.rdom[q], capacity_ * sizeof(unsigned int)));
     }
     CUDA_OK(cudaMalloc(&ps.tgt, capacity_ * sizeof(unsigned long long)));
+    CUDA_OK(cudaMalloc(&ps.queue, capacity_ * sizeof(unsigned int)));
     ps.capacity = capacity_;
     ps.cur = 0;
     ps.pending = 0;
@@ -1134,6 +1128,7 @@ Pool::~Pool() {
                 cudaFree(ps.rdom[q]);
             }
             cudaFree(ps.tgt);
+            cudaFree(ps.queue);
         }
         cudaFree(dstate_);
     }
@@ -1345,19 +1340,22 @@ void Pool::launch_step() {
     if (grid_grow_ == 0) {
         // persistent grids: every resident block slot on the device, grid-stride over the list
         int b1 = 0, b2 = 0;
-        int b3 = 0;
+        int b3 = 0, b4 = 0;
         CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_grow, kBlock, 0));
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_resolve<true>, kBlock, 0));
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_capture, kBlock, 0));
         CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_claim, kBlock, 0));
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, k_neighbours<true>, kBlock, 0));
         grid_grow_ = num_sms_ * std::max(b1, 1);
         grid_capture_ = num_sms_ * std::max(b2, 1);
         grid_claim_ = num_sms_ * std::max(b3, 1);
+        grid_nb_ = num_sms_ * std::max(b4, 1);
     }
     k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
     k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
     k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
-    k_resolve<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
-    launches_ += 4;
+    k_capture<<<grid_capture_, kBlock, 0, st>>>(dstate_);
+    k_neighbours<false><<<grid_nb_, kBlock, 0, st>>>(dstate_);
+    launches_ += 5;
 }
 
 // n cycles in one stream sequence: the begin of cycles 2..n runs in the tail of the previous
@@ -1371,14 +1369,15 @@ void Pool::launch_cycles(int n) {
         return;
     cudaStream_t st = S(stream_);
     k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
-    launches_ += 1 + 3ull * n;
+    launches_ += 1 + 4ull * n;
     for (int q = 0; q < n; q++) {
         k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
         k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
+        k_capture<<<grid_capture_, kBlock, 0, st>>>(dstate_);
         if (q + 1 < n)
-            k_resolve<true><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+            k_neighbours<true><<<grid_nb_, kBlock, 0, st>>>(dstate_);
         else
-            k_resolve<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+            k_neighbours<false><<<grid_nb_, kBlock, 0, st>>>(dstate_);
     }
 }
 
@@ -1419,7 +1418,7 @@ void Pool::step(int n) {
     int full = n / graph_steps_, rest = n % graph_steps_;
     for (int q = 0; q < full; q++)
         CUDA_OK(cudaGraphLaunch((cudaGraphExec_t)graph_exec_, st));
-    launches_ += (unsigned long long)full * (1 + 3ull * graph_steps_);
+    launches_ += (unsigned long long)full * (1 + 4ull * graph_steps_);
     launch_cycles(rest);
     CUDA_OK(cudaGetLastError());
 }
@@ -1463,9 +1462,10 @@ PoolStats Pool::stats() {
         r.nucleated += ps.stat[q][kStatNucleated];
         r.claims += ps.stat[q][kStatClaims];
         r.row_reads += ps.stat[q][kStatRowReads];
-        r.kept += ps.stat[q][kStatKept];
+        r.dropped += ps.stat[q][kStatDropped];
         r.fresh += ps.stat[q][kStatFresh];
         r.rechecks += ps.stat[q][kStatRechecks];
+        r.flagged += ps.stat[q][kStatFlagged];
     }
     return r;
 }
@@ -1487,7 +1487,7 @@ KernelTimes Pool::profile_cycles(int n) {
         ensure_growth(s, slots_[s].steps_launched + 1);
     }
     cudaStream_t st = S(stream_);
-    cudaEvent_t ev[4];
+    cudaEvent_t ev[6];
     for (auto &e : ev)
         CUDA_OK(cudaEventCreate(&e));
     for (int q = 0; q < n; q++) {
@@ -1495,24 +1495,28 @@ KernelTimes Pool::profile_cycles(int n) {
         k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[1], st));
         k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
-        k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[2], st));
-        k_resolve<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+        k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[3], st));
-        CUDA_OK(cudaEventSynchronize(ev[3]));
-        float a, b, c;
-        CUDA_OK(cudaEventElapsedTime(&a, ev[0], ev[1]));
-        CUDA_OK(cudaEventElapsedTime(&b, ev[1], ev[2]));
-        CUDA_OK(cudaEventElapsedTime(&c, ev[2], ev[3]));
-        kt.begin_ms += a;
-        kt.grow_ms += b;
-        kt.capture_ms += c;
+        k_capture<<<grid_capture_, kBlock, 0, st>>>(dstate_);
+        CUDA_OK(cudaEventRecord(ev[4], st));
+        k_neighbours<false><<<grid_nb_, kBlock, 0, st>>>(dstate_);
+        CUDA_OK(cudaEventRecord(ev[5], st));
+        CUDA_OK(cudaEventSynchronize(ev[5]));
+        float t[5];
+        for (int k = 0; k < 5; k++)
+            CUDA_OK(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
+        kt.begin_ms += t[0];
+        kt.grow_ms += t[1];
+        kt.claim_ms += t[2];
+        kt.capture_ms += t[3];
+        kt.neighbours_ms += t[4];
     }
     for (auto &e : ev)
         CUDA_OK(cudaEventDestroy(e));
     kt.cycles = n;
     cycles_launched_ += n;
-    launches_ += 4ull * n;
+    launches_ += 5ull * n;
     return kt;
 }
 

@@ -29,7 +29,7 @@ enum {
     kStatNucleated = 3, // nucleation events
     kStatClaims = 4,    // atomicMin claims issued
     kStatRowReads = 5,  // critical-diagonal-length rows read (diagonal reached the cached minimum)
-    kStatKept = 6,      // records carried into the next list
+    kStatUnused = 6,
     kStatFresh = 7,     // liquid-neighbour masks built from the 26 neighbour types
     kStatRechecks = 8,  // solidification re-checks around claimed cells
     kStatDropped = 9,   // records dropped by the growth pass
@@ -93,6 +93,8 @@ struct PoolState {
     ActiveRec *rec[2];           // active-cell records of the current / next cycle
     unsigned int *rdom[2];       // domain of each record
     unsigned long long *tgt;     // cells claimed this cycle: (domain << 32) | cell
+    unsigned int *queue;         // records the growth pass hands to the claim pass (list positions)
+    unsigned long long qcnt;
     unsigned long long cnt[2];
     unsigned long long tcnt;
     unsigned long long capacity;
@@ -106,18 +108,18 @@ struct PoolState {
     DomainDesc *desc;
     unsigned long long stat[kStatShards][kNumStats];
     unsigned int blocks_done;      // last-block detection of the resolve kernel
-    unsigned long long work[2];    // dynamic chunk counters of the claim and resolve passes
+    unsigned long long work[2];    // spare counters
 };
 
 struct PoolStats {
     unsigned long long cycles; // CA cycles launched
     unsigned long long launches; // kernels launched by step()
-    unsigned long long listed, grown, captured, nucleated, claims, row_reads, kept, fresh, rechecks;
+    unsigned long long listed, grown, captured, nucleated, claims, row_reads, dropped, fresh, rechecks, flagged;
 };
 
 // Per-kernel CUDA-event times of a profiled stretch of cycles.
 struct KernelTimes {
-    double begin_ms = 0, grow_ms = 0, capture_ms = 0; // capture_ms: the claimed-cell pass
+    double begin_ms = 0, grow_ms = 0, claim_ms = 0, capture_ms = 0, neighbours_ms = 0;
     int cycles = 0;
 };
 
@@ -209,7 +211,7 @@ class Pool {
     std::map<std::string, DeviceTables> tables_;
     int num_sms_ = 148;
     unsigned long long cycles_launched_ = 0;
-    int grid_grow_ = 0, grid_capture_ = 0, grid_claim_ = 0;
+    int grid_grow_ = 0, grid_capture_ = 0, grid_claim_ = 0, grid_nb_ = 0;
     unsigned long long launches_ = 0;
     double last_run_ms_ = 0;
     void *census_buf_ = nullptr;

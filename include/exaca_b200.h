@@ -73,9 +73,10 @@ typedef struct {
     uint64_t nucleated; /* nucleation events */
     uint64_t claims;    /* capture claims issued */
     uint64_t row_reads; /* critical-diagonal-length rows read (diagonal reached the cached minimum) */
-    uint64_t kept;      /* list entries carried to the next cycle */
+    uint64_t dropped;   /* active-cell records dropped (solidified, or their domain finished) */
     uint64_t fresh;     /* liquid-neighbour masks built from the 26 neighbour types */
     uint64_t rechecks;  /* solidification re-checks next to claimed cells */
+    uint64_t flagged;   /* records handed from the growth pass to the claim pass */
 } exaca_pool_stats_t;
 
 /* The reference's every-1000-cycle census (src/CAupdate.cpp:738-808). */
@@ -131,7 +132,8 @@ int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cyc
 /* CUDA-event device time (ms) of the last exaca_pool_run_plain on this pool. */
 double exaca_pool_last_run_ms(exaca_pool *pool);
 /* Runs n_cycles cycles kernel by kernel with CUDA events around each launch (no graph) and returns
- * the summed times in kernel_ms[3] = {cycle start + nucleation, growth + claims, capture + list}. */
+ * the summed times in kernel_ms[5] = {cycle start + nucleation, growth pass, claim pass, capture
+ * pass, neighbour pass}. */
 int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms);
 /* Device->host copy of GrainID and CellType (src/runCA.cpp:423-424); NULL skips a field. */
 int exaca_pool_copy_out(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *cell_type);
