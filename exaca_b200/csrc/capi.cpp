@@ -28,17 +28,6 @@ int fail(int code, const std::string &msg) {
     return code;
 }
 
-int classify(const std::exception &e) {
-    std::string m = e.what();
-    if (m.find("not supported") != std::string::npos)
-        return EXACA_ERR_UNSUPPORTED;
-    if (m.find("CUDA") != std::string::npos || m.find("device error") != std::string::npos)
-        return EXACA_ERR_CUDA;
-    if (m.find("admission refused") != std::string::npos)
-        return EXACA_ERR_BUDGET;
-    return EXACA_ERR_INPUT;
-}
-
 template <class F> int guarded(F &&f) {
     try {
         f();
@@ -50,8 +39,20 @@ template <class F> int guarded(F &&f) {
     catch (const std::out_of_range &e) {
         return fail(EXACA_ERR_INPUT, std::string("number out of range in input: ") + e.what());
     }
+    catch (const exaca::Unsupported &e) {
+        return fail(EXACA_ERR_UNSUPPORTED, e.what());
+    }
+    catch (const exaca::AdmissionRefused &e) {
+        return fail(EXACA_ERR_BUDGET, e.what());
+    }
+    catch (const exaca::DeviceError &e) {
+        return fail(EXACA_ERR_CUDA, e.what());
+    }
+    catch (const std::bad_alloc &e) {
+        return fail(EXACA_ERR_BUDGET, "host allocation failed");
+    }
     catch (const std::exception &e) {
-        return fail(classify(e), e.what());
+        return fail(EXACA_ERR_INPUT, e.what());
     }
     catch (...) {
         return fail(EXACA_ERR_INPUT, "unknown error");

@@ -41,7 +41,7 @@ namespace exaca {
     do {                                                                                                               \
         cudaError_t e__ = (x);                                                                                         \
         if (e__ != cudaSuccess)                                                                                        \
-            throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(e__) + " at " #x);              \
+            throw DeviceError(std::string("CUDA error ") + cudaGetErrorString(e__) + " at " #x);                     \
     } while (0)
 
 __constant__ int c_nx[26];
@@ -1011,7 +1011,7 @@ void pin_problem(Problem &p) {
             return;
         cudaError_t e = cudaHostRegister(ptr, bytes, cudaHostRegisterDefault);
         if (e != cudaSuccess && e != cudaErrorHostMemoryAlreadyRegistered)
-            throw std::runtime_error(std::string("CUDA error ") + cudaGetErrorString(e) + " at cudaHostRegister");
+            throw DeviceError(std::string("CUDA error ") + cudaGetErrorString(e) + " at cudaHostRegister");
         cudaGetLastError();
     };
     reg(p.cell_type.data(), p.cell_type.size());
@@ -1160,7 +1160,7 @@ void Pool::ensure_growth(int slot, long long needed) {
         return;
     long long len = std::max<long long>(needed + 1, std::max<long long>(2LL * s.growth_len, 4096));
     if (len > INT_MAX / 2)
-        throw std::runtime_error("growth table too long");
+        throw Unsupported("growth table too long");
     std::vector<double> g;
     build_growth_table(*s.problem, (int)len, g);
     double *d = nullptr;
@@ -1186,10 +1186,10 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     CUDA_OK(cudaSetDevice(device_));
     const Problem &p = *pp;
     if (p.g.zbound_low != 0)
-        throw std::runtime_error("active window must start at z = 0");
+        throw Unsupported("active window must start at z = 0");
     size_t need = slot_bytes(p);
     if (bytes_in_use_ + need > budget_)
-        throw std::runtime_error("admission refused: HBM budget exceeded");
+        throw AdmissionRefused("admission refused: HBM budget exceeded");
     int slot = -1;
     for (int s = 0; s < (int)slots_.size(); s++)
         if (!slots_[s].used) {
@@ -1198,7 +1198,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
         }
     if (slot < 0) {
         if ((int)slots_.size() >= max_domains_)
-            throw std::runtime_error("admission refused: too many domains");
+            throw AdmissionRefused("admission refused: too many domains");
         slot = (int)slots_.size();
         slots_.emplace_back();
         host_desc_.emplace_back();
@@ -1388,7 +1388,7 @@ void Pool::build_graph() {
     cudaStream_t st = S(stream_);
     cudaGraph_t graph;
     if (grid_grow_ == 0)
-        throw std::runtime_error("grids not sized before graph capture");
+        throw DeviceError("grids not sized before graph capture");
     CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
     launch_cycles(graph_steps_);
     CUDA_OK(cudaStreamEndCapture(st, &graph));
@@ -1548,7 +1548,7 @@ void Pool::set_cycle(int slot, int cycle) {
     DomainDesc &h = host_desc_[slot];
     if (cycle > h.cycle) {
         if (h.n_jumps >= kMaxJumps)
-            throw std::runtime_error("too many cycle jumps");
+            throw Unsupported("too many cycle jumps");
         h.jump_lo[h.n_jumps] = h.cycle;
         h.jump_hi[h.n_jumps] = cycle;
         h.n_jumps++;
@@ -1622,7 +1622,7 @@ int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_
         if (d.error || perr) {
             std::ostringstream e;
             e << "device error flags: domain " << d.error << " pool " << perr;
-            throw std::runtime_error(e.str());
+            throw DeviceError(e.str());
         }
         cycle = d.cycle;
         Census c = census(slot);

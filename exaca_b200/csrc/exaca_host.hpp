@@ -25,6 +25,19 @@ enum CellTypeCode : int8_t {
 
 constexpr int kNumOrientations = 10000; // src/runCA.cpp:133
 
+// A valid input this solver does not handle (problem type R, several layers, substrate files).
+struct Unsupported : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+// The HBM budget or slot table of a pool cannot take a problem.
+struct AdmissionRefused : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+// A CUDA runtime error or a device-side error flag.
+struct DeviceError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
 // Every value the reference reads from an input file and its material file
 // (src/CAinitialize.cpp:232-576). Units follow the reference: deltax and deltat in SI.
 struct InputConfig {

@@ -451,13 +451,13 @@ void initialize_problem(Problem &p, std::string &log) {
     auto t0 = std::chrono::steady_clock::now();
     InputConfig &c = p.cfg;
     if (c.simulation_type == "R")
-        throw std::runtime_error("Problem type R (temperature data from files) is not supported by the B200 solver");
+        throw Unsupported("Problem type R (temperature data from files) is not supported by the B200 solver");
     if (c.simulation_type != "C" && c.simulation_type != "S")
         throw std::runtime_error("Unknown problem type \"" + c.simulation_type + "\"");
     if (c.number_of_layers != 1)
-        throw std::runtime_error("The B200 solver supports single-layer problems only (Number of layers: 1)");
+        throw Unsupported("The B200 solver supports single-layer problems only (Number of layers: 1)");
     if (c.simulation_type == "S" && c.use_substrate_file)
-        throw std::runtime_error("Substrate files are not supported by the B200 solver");
+        throw Unsupported("Substrate files are not supported by the B200 solver");
 
     int it[9][26], lens[9];
     build_itlist(it, lens);
@@ -468,7 +468,7 @@ void initialize_problem(Problem &p, std::string &log) {
     log += "================================================================\n";
     log += "Mesh initialized\n";
     if ((long)g.mx * g.my * g.nz > 2000000000L)
-        throw std::runtime_error("domain too large: the cell index must fit in 31 bits");
+        throw Unsupported("domain too large: the cell index must fit in 31 bits");
 
     p.cts.assign(g.domain_size, 0);
     p.layer_id.assign(g.domain_size, 0);
@@ -518,7 +518,7 @@ void initialize_problem(Problem &p, std::string &log) {
         if (common == 0.0f)
             common = v;
         else if (v != common)
-            throw std::runtime_error("non-uniform UndercoolingChange is not supported by the B200 solver");
+            throw Unsupported("non-uniform UndercoolingChange is not supported by the B200 solver");
     }
     p.du_value = common;
     p.voronoi_seeds = seeds;

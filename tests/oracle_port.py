@@ -1,0 +1,66 @@
+"""ctypes binding of the CPU restatement oracle (oracle/_port/liboracle.so). Test infrastructure."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB = os.path.join(ROOT, "oracle", "_port", "liboracle.so")
+DATA = os.path.join(ROOT, "exaca_b200", "data")
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB) or os.path.getmtime(LIB) < os.path.getmtime(os.path.join(ROOT, "oracle", "exaca_oracle.cpp")):
+            subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "port"], check=True, capture_output=True)
+        L = ctypes.CDLL(LIB)
+        L.oracle_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+        L.oracle_create.restype = ctypes.c_void_p
+        L.oracle_error.restype = ctypes.c_char_p
+        L.oracle_free.argtypes = [ctypes.c_void_p]
+        L.oracle_geometry.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]
+        L.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+        L.oracle_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_cycle.argtypes = [ctypes.c_void_p]
+        L.oracle_fields.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 5
+        _lib = L
+    return _lib
+
+
+class Oracle:
+    def __init__(self, input_file):
+        self.h = lib().oracle_create(os.fsencode(input_file), os.fsencode(DATA))
+        if not self.h:
+            raise RuntimeError(lib().oracle_error().decode())
+        g = (ctypes.c_longlong * 6)()
+        lib().oracle_geometry(self.h, g)
+        self.mx, self.my, self.nz, self.nz_active, self.n, self.na = list(g)
+
+    def step(self, n):
+        lib().oracle_step(self.h, n)
+
+    def run(self):
+        c = ctypes.c_int()
+        lib().oracle_run(self.h, ctypes.byref(c))
+        return c.value
+
+    @property
+    def cycle(self):
+        return lib().oracle_cycle(self.h)
+
+    def fields(self):
+        ct = np.empty(self.n, np.int32)
+        gid = np.empty(self.n, np.int32)
+        dl = np.empty(self.na, np.float32)
+        doc = np.empty(3 * self.na, np.float32)
+        cdl = np.empty(26 * self.na, np.float32)
+        lib().oracle_fields(self.h, *(a.ctypes.data_as(ctypes.c_void_p) for a in (ct, gid, dl, doc, cdl)))
+        return dict(cell_type=ct, grain_id=gid, dl=dl, doc=doc, cdl=cdl)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().oracle_free(self.h)
+            self.h = None
