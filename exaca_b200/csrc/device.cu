@@ -236,7 +236,9 @@ __device__ __forceinline__ long long domain_liquid(const DomainDesc &D) {
 // ---------------------------------------------------------------------------------------------
 // Capture of liquid cell t by active cell c through neighbour direction l
 // (src/CAupdate.cpp:353-563, 713-717).
-__device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int t, int l) {
+// Warp-cooperative: every lane evaluates the (identical) geometry in lock step, then lane n < 26
+// computes critical length n; lane 0 writes the scalar state. Returns the new DiagonalLength.
+__device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int t, int l, int lane) {
     // all loads first: capturer state, then its orientation
     const int h = D.gid[c];
     const float docx = D.doc[3ull * c + 0], docy = D.doc[3ull * c + 1], docz = D.doc[3ull * c + 2];
@@ -314,17 +316,19 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     double L12 = 0.5 * (dmin(I1, sqrt3) + dmin(I2, sqrt3));
     double L13 = 0.5 * (dmin(J1, sqrt3) + dmin(J2, sqrt3));
     double NewODiagL = sqrt(2.0) * dmax(L12, L13);
-    D.gid[t] = h;
-    D.dl[t] = (float)NewODiagL;
     double cd0 = xc - cxold, cd1 = yc - cyold, cd2 = zc - czold;
     double nd = sqrt(cd0 * cd0 + cd1 * cd1 + cd2 * cd2);
     double uv0 = cd0 / nd, uv1 = cd1 / nd, uv2 = cd2 / nd;
     double cx = xc - NewODiagL * uv0;
     double cy = yc - NewODiagL * uv1;
     double cz = zc - NewODiagL * uv2;
-    D.doc[3 * t + 0] = (float)cx;
-    D.doc[3 * t + 1] = (float)cy;
-    D.doc[3 * t + 2] = (float)cz;
+    if (lane == 0) {
+        D.gid[t] = h;
+        D.dl[t] = (float)NewODiagL;
+        D.doc[3ull * t + 0] = (float)cx;
+        D.doc[3ull * t + 1] = (float)cy;
+        D.doc[3ull * t + 2] = (float)cz;
+    }
     // face normals: float sums of the unit-vector components (src/CAupdate.cpp:526-551)
     double Fx[4], Fy[4], Fz[4];
     Fx[0] = g0 + g3 + g6;
@@ -339,9 +343,8 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     Fz[1] = g2 - g5 + g8;
     Fz[2] = g2 + g5 - g8;
     Fz[3] = g2 - g5 - g8;
-    float *out = D.cdl + 26 * t;
-#pragma unroll 2
-    for (int n = 0; n < 26; n++) {
+    if (lane < 26) {
+        const int n = lane;
         double a0 = xp + c_nx[n] - cx;
         double b0 = yp + c_ny[n] - cy;
         double d0 = zp + c_nz[n] - cz;
@@ -350,7 +353,7 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
         double q2 = a0 * Fx[2] + b0 * Fy[2] + d0 * Fz[2];
         double q3 = a0 * Fx[3] + b0 * Fy[3] + d0 * Fz[3];
         double m = dmax(dmax(fabs(q0), fabs(q1)), dmax(fabs(q2), fabs(q3)));
-        out[n] = (float)m;
+        D.cdl[26ull * t + n] = (float)m;
     }
     return (float)NewODiagL;
 }
@@ -659,8 +662,17 @@ __global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
     const unsigned int *rdom = P->rdom[lst];
     DomainDesc *desc = P->desc;
     unsigned long long st_claims = 0, st_rows = 0, st_fresh = 0, st_dropped = 0;
-    for (unsigned long long qi = (unsigned long long)blockIdx.x * kBlock + threadIdx.x; qi < nq;
-         qi += (unsigned long long)gridDim.x * kBlock) {
+    const unsigned long long nthreads = (unsigned long long)gridDim.x * kBlock;
+    const unsigned long long me = (unsigned long long)threadIdx.x * gridDim.x + blockIdx.x;
+    // block-uniform loop (block_reserve_on); consecutive items on different blocks
+    for (unsigned long long q0 = 0; q0 < nq; q0 += nthreads) {
+        const unsigned long long qi = q0 + me;
+        unsigned int first = 0, pushed_dom = 0;
+        unsigned int pushed_cell = 0;
+        int first_plane = 0, first_my = 0;
+        do {
+        if (qi >= nq)
+            break;
         const unsigned long long i = P->queue[qi];
         const ActiveRec rec = recs[i];
         if (rec.cell == kTombstone || __float_as_uint(rec.cdl_min) != kNeedsClaim)
@@ -723,7 +735,6 @@ __global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
             // this cycle lists it for k_capture / k_neighbours
             const unsigned long long key = ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
             const unsigned int want = 0xffffffffu - D.epoch;
-            unsigned int first = 0;
 #pragma unroll
             for (int l = 0; l < 26; l++) {
                 if (reach & (1u << l)) {
@@ -733,11 +744,20 @@ __global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
                 }
             }
             st_claims += __popc(reach);
+            pushed_dom = dom;
+            pushed_cell = c;
+            first_plane = plane;
+            first_my = my;
+        }
+        } while (false);
+        // list the cells this thread claimed first (block-aggregated reservation)
+        const unsigned long long pos = block_reserve_on(&P->tcnt, P->capacity, &P->error, __popc(first));
+        if (pos != ULLONG_MAX) {
+            unsigned long long k = pos;
             for (unsigned int bits = first; bits; bits &= bits - 1) {
                 int l = __ffs(bits) - 1;
-                unsigned long long pos = warp_reserve(&P->tcnt, P->capacity, &P->error);
-                if (pos != ULLONG_MAX)
-                    P->tgt[pos] = ((unsigned long long)dom << 32) | (unsigned int)((long long)c + nb_offset(l, plane, my));
+                P->tgt[k++] = ((unsigned long long)pushed_dom << 32) |
+                              (unsigned int)((long long)pushed_cell + nb_offset(l, first_plane, first_my));
             }
         }
     }
@@ -760,10 +780,20 @@ __global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
 __global__ void __launch_bounds__(kBlock) k_capture(PoolState *P) {
     const int app = P->pending; // list of the next cycle
     const unsigned long long T = P->tcnt;
+    // claimed cell j gets record slot base + j (the count grows by T in k_neighbours)
+    const unsigned long long base = P->cnt[app];
+    if (base + T > P->capacity) {
+        if (threadIdx.x == 0 && blockIdx.x == 0)
+            atomicOr(&P->error, kErrListOverflow);
+        return;
+    }
     DomainDesc *desc = P->desc;
+    const int lane = threadIdx.x & 31;
+    // one warp per claimed cell, consecutive cells on different blocks (spread over all SMs)
+    const unsigned long long nwarps = (unsigned long long)gridDim.x * (kBlock / 32);
+    const unsigned long long w0 = (unsigned long long)(threadIdx.x >> 5) * gridDim.x + blockIdx.x;
     unsigned long long st_cap = 0;
-    for (unsigned long long j = (unsigned long long)blockIdx.x * kBlock + threadIdx.x; j < T;
-         j += (unsigned long long)gridDim.x * kBlock) {
+    for (unsigned long long j = w0; j < T; j += nwarps) {
         const unsigned long long e = P->tgt[j];
         const unsigned int dom = (unsigned int)(e >> 32);
         const unsigned int t = (unsigned int)e;
@@ -774,32 +804,40 @@ __global__ void __launch_bounds__(kBlock) k_capture(PoolState *P) {
         cell_coords(D, w, wx, wy, wz);
         cell_coords(D, t, tx, ty, tz);
         const int l = c_dir[(tz - wz + 1) * 9 + (tx - wx + 1) * 3 + (ty - wy + 1)];
-        const float new_dl = capture_cell(D, w, t, l);
-        D.lmask[t] = kMaskFresh;
-        unsigned long long pos = warp_reserve(&P->cnt[app], P->capacity, &P->error);
-        if (pos != ULLONG_MAX) {
+        const float new_dl = capture_cell(D, w, t, l, lane);
+        __syncwarp();
+        if (lane == 0) {
+            D.lmask[t] = kMaskFresh;
             ActiveRec r;
             r.cell = t;
             r.dl = new_dl;
             r.cdl_min = 0.0f;
             r.cts = cts_t;
-            P->rec[app][pos] = r;
-            P->rdom[app][pos] = dom;
+            P->rec[app][base + j] = r;
+            P->rdom[app][base + j] = dom;
+            // read as active only from the next kernel on, after the octahedron data is written
+            D.ctype[t] = kActive;
+            atomicAdd((unsigned long long *)&D.liquid_shard[(blockIdx.x + j) & (kLiquidShards - 1)],
+                      (unsigned long long)(-1ll));
+            st_cap++;
         }
-        // the captured cell becomes active only after its octahedron data is written
-        D.ctype[t] = kActive;
-        atomicAdd((unsigned long long *)&D.liquid_shard[blockIdx.x & (kLiquidShards - 1)], (unsigned long long)(-1ll));
-        st_cap++;
     }
     block_stats(P, st_cap, 0, kStatCaptured, kStatCaptured);
 }
 
 template <bool kTail> __global__ void __launch_bounds__(kBlock) k_neighbours(PoolState *P) {
     const unsigned long long n = P->tcnt * 26ull;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        // the records k_capture wrote at fixed slots join the next cycle's list
+        const int app = P->pending;
+        if (P->cnt[app] + P->tcnt <= P->capacity)
+            P->cnt[app] += P->tcnt;
+    }
     DomainDesc *desc = P->desc;
     unsigned long long st_rc = 0;
-    for (unsigned long long j = (unsigned long long)blockIdx.x * kBlock + threadIdx.x; j < n;
-         j += (unsigned long long)gridDim.x * kBlock) {
+    // consecutive items on different blocks (spread over all SMs)
+    const unsigned long long nthreads = (unsigned long long)gridDim.x * kBlock;
+    for (unsigned long long j = (unsigned long long)threadIdx.x * gridDim.x + blockIdx.x; j < n; j += nthreads) {
         const unsigned long long q = j / 26ull;
         const int l = (int)(j - q * 26ull);
         const unsigned long long e = P->tgt[q];
