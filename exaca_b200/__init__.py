@@ -81,6 +81,17 @@ class CensusT(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in ("superheated", "undercooled", "active", "solid", "remaining", "next_cts")]
 
 
+class CellFieldsT(ctypes.Structure):
+    """exaca_cell_fields: device pointers to one domain's CellType / LayerID / CritTimeStep."""
+    _fields_ = [
+        ("cell_type", ctypes.c_void_p), ("layer_id", ctypes.c_void_p), ("crit_time_step", ctypes.c_void_p),
+        ("domain_size", ctypes.c_int64), ("active_size", ctypes.c_int64), ("cycle", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+    ]
+
+
+CENSUS_MAX_DOMAINS = 256
+
 # Every symbol include/exaca_b200.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -109,6 +120,7 @@ SIGNATURES = {
     "exaca_pool_last_run_ms": ([_P], ctypes.c_double),
     "exaca_pool_profile_cycles": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_problem_pin": ([_P], _I),
+    "exaca_census_cells": ([_I, _P, ctypes.POINTER(CellFieldsT), _I, ctypes.POINTER(CensusT)], _I),
 }
 
 _lib = None
@@ -141,6 +153,22 @@ def _ptr(a: np.ndarray | None):
 def run_program(input_file: str, device: int = 0) -> None:
     """RunProgram_Reduced at one rank (src/runCA.cpp:19-461): solve an input file, write outputs."""
     _check(load_library().exaca_run_program(os.fsencode(input_file), device))
+
+
+def census_cells(device: int, domains: list, stream: int = 0) -> list:
+    """exaca_census_cells: IntermediateOutputAndCheck's census (src/CAupdate.cpp:738-808) of cell
+    fields already in device memory, without allocating device memory. Each domain is a dict with
+    the device addresses (ints) "cell_type" (int8), "layer_id" (int8), "crit_time_step" (int32) and
+    "domain_size", "active_size", "cycle"; at most CENSUS_MAX_DOMAINS per call. `stream` is a
+    cudaStream_t handle (0: the legacy default stream); the call waits for it."""
+    n = len(domains)
+    arr = (CellFieldsT * max(n, 1))()
+    for i, d in enumerate(domains):
+        arr[i] = CellFieldsT(d["cell_type"], d["layer_id"], d["crit_time_step"], d["domain_size"],
+                             d["active_size"], d["cycle"], 0)
+    out = (CensusT * max(n, 1))()
+    _check(load_library().exaca_census_cells(device, ctypes.c_void_p(stream), arr, n, out))
+    return [{k: getattr(out[i], k) for k, _ in CensusT._fields_} for i in range(n)]
 
 
 # Inconel625 material values (the material file shipped under data/Materials)

@@ -21,7 +21,7 @@ OBJ = os.path.join(HERE, "_build")
 ROOT = os.path.dirname(HERE)
 
 HOST_SOURCES = ["input.cpp", "init.cpp", "output.cpp", "capi.cpp"]
-CUDA_SOURCES = ["device.cu"]
+CUDA_SOURCES = ["device.cu", "census_scratch.cu"]
 HEADERS = ["exaca_host.hpp", "pool.hpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]

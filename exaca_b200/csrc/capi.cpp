@@ -91,6 +91,11 @@ void write_outputs(const exaca::Problem &p, const int32_t *gid, const std::strin
 
 } // namespace
 
+namespace exaca {
+void census_cells(int device, void *stream, const exaca_cell_fields *domains, int n_domains, exaca_census *out);
+int census_device_count();
+} // namespace exaca
+
 extern "C" {
 
 const char *exaca_last_error(void) { return g_last_error.c_str(); }
@@ -280,6 +285,28 @@ int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c) {
         c->remaining = k.remaining;
         c->next_cts = k.next_cts;
     });
+}
+
+int exaca_census_cells(int device, void *stream, const exaca_cell_fields *domains, int n_domains, exaca_census *out) {
+    if (n_domains < 0 || n_domains > EXACA_CENSUS_MAX_DOMAINS)
+        return fail(EXACA_ERR_ARG, "n_domains " + std::to_string(n_domains) + " outside 0.." +
+                                       std::to_string(EXACA_CENSUS_MAX_DOMAINS) +
+                                       " (the fixed census scratch holds at most that many domains)");
+    if (n_domains == 0)
+        return EXACA_OK;
+    if (!domains || !out)
+        return fail(EXACA_ERR_ARG, "null domains or out");
+    for (int i = 0; i < n_domains; i++) {
+        const exaca_cell_fields &d = domains[i];
+        if (d.domain_size < 0 || d.active_size < 0 || d.active_size > d.domain_size)
+            return fail(EXACA_ERR_ARG, "domain " + std::to_string(i) + ": bad domain_size / active_size");
+        if (d.domain_size > 0 && (!d.cell_type || !d.layer_id || !d.crit_time_step))
+            return fail(EXACA_ERR_ARG, "domain " + std::to_string(i) + ": null field pointer");
+    }
+    const int ndev = exaca::census_device_count();
+    if (device < 0 || device >= ndev)
+        return fail(EXACA_ERR_ARG, "bad device " + std::to_string(device));
+    return guarded([&] { exaca::census_cells(device, stream, domains, n_domains, out); });
 }
 
 int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cycle) {

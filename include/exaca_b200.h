@@ -146,6 +146,33 @@ int64_t exaca_pool_bytes_in_use(exaca_pool *pool);
 /* Writes the reference's output files for a finished slot (src/CAprint.cpp:170-571). */
 int exaca_pool_write_outputs(exaca_pool *pool, int slot, const exaca_problem *p, const char *path_prefix);
 
+/* ---- Census without device allocation (no counterpart in the reference) ----
+ * The census of IntermediateOutputAndCheck (src/CAupdate.cpp:738-808) computed over cell fields that
+ * the caller holds in device memory, for callers that must not allocate device memory: a monitor
+ * sampling solves that are still running (cudaMalloc / cudaFree may synchronise the device and
+ * stall them) or a server whose HBM budget is fully handed out. It allocates nothing: its working
+ * data lives in a fixed 24 KiB array in the library's device image (per device), which holds the
+ * descriptors and accumulators of at most EXACA_CENSUS_MAX_DOMAINS domains per call; larger
+ * n_domains returns EXACA_ERR_ARG. Each field pointer is a CUDA device pointer on `device`, indexed
+ * like the pool's fields (k*mx*my + i*my + j); cell_type holds the reference's codes. */
+#define EXACA_CENSUS_MAX_DOMAINS 256
+typedef struct {
+    const int8_t *cell_type;       /* domain_size cells */
+    const int8_t *layer_id;        /* domain_size cells */
+    const int32_t *crit_time_step; /* domain_size cells */
+    int64_t domain_size;           /* cells */
+    int64_t active_size;           /* cells of the active window (next_cts is taken over these) */
+    int32_t cycle;                 /* the CA cycle the census is taken at */
+    int32_t reserved;              /* 0 */
+} exaca_cell_fields;
+/* Writes out[i] for domains[i], i < n_domains, equal to what exaca_pool_census reports for a slot
+ * holding the same fields at the same cycle. `stream` is a cudaStream_t (NULL: the legacy default
+ * stream); the call waits for it before returning. The first call on a device looks up the scratch
+ * array's device address and loads the kernel; make that first call before any stream capture.
+ * All calls on a device share the scratch array: a per-device lock keeps calls from several host
+ * threads from overlapping on it. */
+int exaca_census_cells(int device, void *stream, const exaca_cell_fields *domains, int n_domains, exaca_census *out);
+
 #ifdef __cplusplus
 }
 #endif
