@@ -119,6 +119,8 @@ SIGNATURES = {
     "exaca_pool_write_outputs": ([_P, _I, _P, ctypes.c_char_p], _I),
     "exaca_pool_last_run_ms": ([_P], ctypes.c_double),
     "exaca_pool_profile_cycles": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
+    "exaca_pool_timed_step": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
+    "exaca_pool_profile_persistent": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_problem_pin": ([_P], _I),
     "exaca_census_cells": ([_I, _P, ctypes.POINTER(CellFieldsT), _I, ctypes.POINTER(CensusT)], _I),
 }
@@ -294,10 +296,23 @@ class Pool:
         return float(load_library().exaca_pool_last_run_ms(self._h))
 
     def profile_cycles(self, n_cycles: int) -> dict:
-        """Runs n cycles kernel by kernel with CUDA events around each launch; summed ms per kernel."""
-        t = (ctypes.c_double * 5)()
+        """n_cycles cycles pass by pass as separate kernels; summed CUDA-event ms per pass."""
+        t = (ctypes.c_double * 4)()
         _check(load_library().exaca_pool_profile_cycles(self._h, n_cycles, t))
-        return {"k_step_begin": t[0], "k_grow": t[1], "k_claim": t[2], "k_capture": t[3], "k_neighbours": t[4]}
+        return {"k_step_begin": t[0], "k_grow": t[1], "k_claim": t[2], "k_capture_pass": t[3]}
+
+    def profile_persistent(self, n_cycles: int) -> dict:
+        """step(n_cycles) with the persistent kernel's timeline on; per-cycle averages (us)."""
+        t = (ctypes.c_double * 7)()
+        _check(load_library().exaca_pool_profile_persistent(self._h, n_cycles, t))
+        return {"grow_first": t[0], "grow_last": t[1], "claim_first": t[2], "claim_last": t[3], "capture_first": t[4],
+                "capture_last": t[5], "cycle_end_and_start": t[6]}
+
+    def timed_step(self, n_cycles: int) -> float:
+        """step(n_cycles) (one persistent launch) timed with CUDA events; waits; returns ms."""
+        ms = ctypes.c_double()
+        _check(load_library().exaca_pool_timed_step(self._h, n_cycles, ctypes.byref(ms)))
+        return ms.value
 
     def retire(self, slot: int) -> None:
         _check(load_library().exaca_pool_retire(self._h, slot))

@@ -262,8 +262,19 @@ int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms)
         kernel_ms[1] = t.grow_ms;
         kernel_ms[2] = t.claim_ms;
         kernel_ms[3] = t.capture_ms;
-        kernel_ms[4] = t.neighbours_ms;
     });
+}
+
+int exaca_pool_profile_persistent(exaca_pool *pool, int n_cycles, double *us) {
+    if (!pool || !us || n_cycles < 0)
+        return fail(EXACA_ERR_ARG, "bad argument");
+    return guarded([&] { pool->pool->profile_persistent(n_cycles, us); });
+}
+
+int exaca_pool_timed_step(exaca_pool *pool, int n_cycles, double *ms) {
+    if (!pool || !ms || n_cycles < 0)
+        return fail(EXACA_ERR_ARG, "bad argument");
+    return guarded([&] { *ms = pool->pool->timed_step(n_cycles); });
 }
 
 int exaca_problem_pin(exaca_problem *p) {

@@ -1,19 +1,21 @@
 // B200 kernels and pool runtime for ExaCA's per-cycle cellular-automaton update.
 //
-// One CA cycle (src/runCA.cpp:290-341; src/CAupdate.cpp:67-728) is three kernels over a pool of
-// domains:
-//   begin (k_step_begin, or the tail of the previous k_neighbours): per domain, the device-side
-//          termination check, cycle/epoch advance and nucleation of the sites whose time has come
-//          (nuclei are pre-sorted by time, one cursor each).
-//   k_grow: streams the 16-byte records of the active cells (shared compacted list): diagonal
+// One CA cycle (src/runCA.cpp:290-341; src/CAupdate.cpp:67-728) is a start and two passes over a
+// pool of domains:
+//   begin_cycle: per domain, the device-side termination check, cycle/epoch advance and nucleation
+//          of the sites whose time has come (nuclei are pre-sorted by time, one cursor each).
+//   grow/claim: streams the 16-byte records of the active cells (shared compacted list): diagonal
 //          growth from the host-built increment table, solidification of cells with no liquid
 //          neighbour, and a 64-bit atomicMin claim (epoch, capturer index) on every liquid neighbour
 //          the octahedron reaches. Liquid neighbours come from a per-cell mask kept up to date by
 //          captures and nucleations; the 26 critical lengths are read only when the diagonal has
 //          reached the cached minimum over the liquid neighbours.
-//   k_capture / k_neighbours: per claimed cell: capture by the lowest-index claimant (new decentred
-//          octahedron, 26 critical lengths), mask updates of its active neighbours, and for those
-//          the solidification re-check.
+//   capture: per claimed cell: capture by the lowest-index claimant (new decentred octahedron, 26
+//          critical lengths), mask updates of its active neighbours, and for those the
+//          solidification re-check.
+// Stretches of cycles run in one persistent cooperative kernel (k_cycles) whose blocks meet at
+// bounded grid-wide barriers between the passes; the last block to reach the end of a cycle
+// starts the next one. The same passes also run as separate kernels (per-pass timing).
 // The claim rule reproduces the Kokkos-Serial loop order exactly: serial visits active cells in
 // ascending index and captures flip Liquid to Active in place, so the capturer of a cell is the
 // lowest-index claimant, and an active cell sees a neighbour as liquid iff it was liquid at the
@@ -28,6 +30,7 @@
 #include <chrono>
 #include <climits>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <sstream>
@@ -64,6 +67,8 @@ constexpr int kErrGrowthTable = 1;
 constexpr int kErrListOverflow = 2;
 constexpr int kErrBounds = 4;
 constexpr int kBlock = 256;
+// rmin2 of a record whose minimum direction is not known: the cached minimum alone applies
+constexpr unsigned long long kNoMin2 = 0xffffffffull << 32;
 
 __device__ __forceinline__ double dmin(double a, double b) { return (b < a) ? b : a; } // std::min
 __device__ __forceinline__ double dmax(double a, double b) { return (a < b) ? b : a; } // std::max
@@ -221,7 +226,6 @@ __device__ void make_fresh_octahedron(const DomainDesc &D, unsigned int c) {
 #pragma unroll
     for (int n = 0; n < 13; n++)
         o[n] = t[n];
-    D.lmask[c] = kMaskFresh;
 }
 
 
@@ -236,12 +240,12 @@ __device__ __forceinline__ long long domain_liquid(const DomainDesc &D) {
 // ---------------------------------------------------------------------------------------------
 // Capture of liquid cell t by active cell c through neighbour direction l
 // (src/CAupdate.cpp:353-563, 713-717).
-// Warp-cooperative: every lane evaluates the (identical) geometry in lock step, then lane n < 26
-// computes critical length n; lane 0 writes the scalar state. Returns the new DiagonalLength.
-__device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int t, int l, int lane) {
-    // all loads first: capturer state, then its orientation
-    const int h = D.gid[c];
-    const float docx = D.doc[3ull * c + 0], docy = D.doc[3ull * c + 1], docz = D.doc[3ull * c + 2];
+// Cooperative over kLanes lanes: every lane of the group evaluates the (identical) geometry, lane
+// `sub` computes critical lengths sub, sub + kLanes, ...; lane 0 of the group writes the scalar
+// state. Returns the new DiagonalLength.
+template <int kLanes>
+__device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int t, int l, int sub, int h, float docx,
+                              float docy, float docz) {
     int rx, ry, rz;
     cell_coords(D, c, rx, ry, rz);
     const int GlobalX = rx + D.xoff, GlobalY = ry + D.yoff, GlobalZ = rz;
@@ -322,7 +326,7 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     double cx = xc - NewODiagL * uv0;
     double cy = yc - NewODiagL * uv1;
     double cz = zc - NewODiagL * uv2;
-    if (lane == 0) {
+    if (sub == 0) {
         D.gid[t] = h;
         D.dl[t] = (float)NewODiagL;
         D.doc[3ull * t + 0] = (float)cx;
@@ -343,8 +347,8 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     Fz[1] = g2 - g5 + g8;
     Fz[2] = g2 + g5 - g8;
     Fz[3] = g2 - g5 - g8;
-    if (lane < 26) {
-        const int n = lane;
+#pragma unroll 1
+    for (int n = sub; n < 26; n += kLanes) {
         double a0 = xp + c_nx[n] - cx;
         double b0 = yp + c_ny[n] - cy;
         double d0 = zp + c_nz[n] - cz;
@@ -358,45 +362,66 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     return (float)NewODiagL;
 }
 
-// A nucleation site stopped being liquid: its active neighbours drop it from their masks.
-__device__ void drop_from_neighbour_masks(const DomainDesc &D, unsigned int t) {
+// A nucleation site stopped being liquid: its active neighbours drop it from their masks. The 26
+// neighbour types are loaded first (invalid directions read the site itself), then the updates go out.
+__device__ void drop_from_neighbour_masks(const DomainDesc &D, unsigned int *rstat, unsigned long long cap,
+                                          unsigned int t) {
     int rx, ry, rz;
     cell_coords(D, t, rx, ry, rz);
     const unsigned int valid = neighbour_mask(D, rx, ry, rz);
     const int plane = D.mx * D.my, my = D.my;
-    for (unsigned int bits = valid; bits; bits &= bits - 1) {
-        int l = __ffs(bits) - 1;
-        unsigned int a = (unsigned int)((long long)t + nb_offset(l, plane, my));
-        if (__ldcg(D.ctype + a) == kActive)
-            atomicAnd(D.lmask + a, ~(1u << c_opp[l]));
+    int8_t nt[26];
+    unsigned int np[26];
+#pragma unroll
+    for (int l = 0; l < 26; l++) {
+        const long long a = (long long)t + ((valid >> l) & 1u ? nb_offset(l, plane, my) : 0);
+        nt[l] = __ldcg(D.ctype + a);
+        np[l] = __ldcg(D.pos + a);
     }
+#pragma unroll
+    for (int l = 0; l < 26; l++)
+        if (((valid >> l) & 1u) && nt[l] == kActive && np[l] < cap)
+            atomicAnd(rstat + np[l], ~(1u << c_opp[l]));
 }
 
 // ---------------------------------------------------------------------------------------------
 // Start of a CA cycle for every domain (src/runCA.cpp:290-298, src/CAupdate.cpp:67-200), run by one
 // block: list swap, device-side termination check, cycle advance, nucleation. Reads that may see
 // data other blocks of the same kernel wrote go through L2 (__ldcg).
-__device__ void begin_cycle(PoolState *P) {
+__device__ __noinline__ void begin_cycle(PoolState *P) {
     __shared__ int s_cur;
-    if (threadIdx.x == 0) {
+    if (threadIdx.x < 32) {
         // the list the previous cycle left becomes current; when it was a compacted copy, the old
-        // one is emptied and carries no dropped records any more
-        int prev = P->cur;
-        int cur = P->pending;
-        if (cur != prev) {
-            P->cnt[prev] = 0;
-            P->tombs = 0;
+        // one is emptied and carries no dropped records any more (all loads issued together)
+        static_assert(kShards == 32, "one lane per shard");
+        const int lane = threadIdx.x;
+        unsigned long long added = P->tomb_s[lane].v;
+        P->tomb_s[lane].v = 0;
+        P->qcnt_s[lane].v = 0;
+        P->tcnt_s[lane].v = 0;
+#pragma unroll
+        for (int o = 16; o; o >>= 1)
+            added += __shfl_down_sync(0xffffffffu, added, o);
+        if (lane == 0) {
+            const int prev = P->cur;
+            const int cur = P->pending;
+            const unsigned long long cnt0 = P->cnt[0], cnt1 = P->cnt[1];
+            unsigned long long tombs = P->tombs + added;
+            const unsigned long long cnt_cur = cur ? cnt1 : cnt0;
+            if (cur != prev) {
+                P->cnt[prev] = 0;
+                tombs = 0;
+            }
+            P->tombs = tombs;
+            P->cur = cur;
+            // compact when dropped records exceed an eighth of the list
+            int compact = tombs * 8 > cnt_cur ? 1 : 0;
+            P->compact = compact;
+            P->pending = compact ? cur ^ 1 : cur;
+            if (compact)
+                P->cnt[cur ^ 1] = 0;
+            s_cur = cur;
         }
-        P->cur = cur;
-        // compact when dropped records exceed an eighth of the list
-        int compact = P->tombs * 8 > P->cnt[cur] ? 1 : 0;
-        P->compact = compact;
-        P->pending = compact ? cur ^ 1 : cur;
-        if (compact)
-            P->cnt[cur ^ 1] = 0;
-        P->tcnt = 0;
-        P->qcnt = 0;
-        s_cur = cur;
     }
     __syncthreads();
     const int cur = s_cur;
@@ -450,12 +475,15 @@ __device__ void begin_cycle(PoolState *P) {
                     r.cts = D.cts[loc];
                     P->rec[cur][pos] = r;
                     P->rdom[cur][pos] = (unsigned int)d;
+                    P->rstat[cur][pos] = kMaskFresh;
+                    P->rmin2[cur][pos] = kNoMin2;
+                    D.pos[loc] = (unsigned int)pos;
                 }
                 D.ctype[loc] = kActive;
             }
             __syncwarp();
             if (fire)
-                drop_from_neighbour_masks(D, loc);
+                drop_from_neighbour_masks(D, P->rstat[cur], P->capacity, loc);
             unsigned int fired = __ballot_sync(0xffffffffu, fire);
             fired_total += __popc(fired);
             cursor += n_due;
@@ -476,31 +504,50 @@ __device__ void begin_cycle(PoolState *P) {
 __global__ void k_step_begin(PoolState *P) { begin_cycle(P); }
 
 // ---------------------------------------------------------------------------------------------
-// Per-cycle growth of the active cells, split by cost:
-//   k_grow    streams every record (kBatch per thread, loads issued first): eligibility, diagonal
-//             growth (src/CAupdate.cpp:257-261), drop of finished / re-check-solidified cells, and
-//             solidification of cells whose liquid mask is empty. A record whose mask must still
-//             be built, or whose diagonal reached the cached minimum critical length, is flagged
-//             (cdl_min = kNeedsClaim) for
-//   k_claim   one thread per flagged record, chunks handed out dynamically: the liquid mask from
-//             the 26 neighbour types, the critical-length row (13 aligned 8-byte loads), and the
-//             claims (src/CAupdate.cpp:320-352).
+// One CA cycle after its start (begin_cycle) is three passes over the pool:
+//   grow        every record of the current list (kBatch per lane, loads issued first): eligibility
+//               and diagonal growth (src/CAupdate.cpp:257-261), drop of finished or
+//               re-check-solidified cells, solidification of cells whose liquid mask is empty. A
+//               record whose mask must still be built, or whose diagonal reached the cached minimum
+//               critical length, goes to the claim queue.
+//   claim       one queue entry per thread: the liquid mask from the 26 neighbour types, the
+//               critical-length row (13 aligned 8-byte loads) and the claims (src/CAupdate.cpp:
+//               320-352); every claim is listed.
+//   capture     kCaptureLanes lanes per listed claim: the winner's group captures the cell
+//               (src/CAupdate.cpp:353-563) and re-checks the captured cell's active neighbours.
+// They run as three kernels per cycle (k_grow, k_claim, k_capture_pass) or, for stretches of
+// cycles, inside the persistent cooperative kernel k_cycles with grid-wide barriers between them.
 constexpr unsigned int kNeedsClaim = 0xffffffffu; // NaN pattern in ActiveRec::cdl_min
 constexpr int kBatch = 4;
+constexpr int kCaptureLanes = 8;
+constexpr int kErrBarrier = 8;
 
-struct GrowStats {
-    unsigned long long listed = 0, grown = 0, dropped = 0, flagged = 0;
+struct CycleStats {
+    unsigned long long listed = 0, grown = 0, dropped = 0, flagged = 0, claims = 0, rows = 0, fresh = 0,
+                       captured = 0, rechecks = 0;
 };
+
+__device__ void flush_stats(PoolState *P, const CycleStats &st) {
+    block_stats(P, st.listed, st.grown, kStatListed, kStatGrown);
+    block_stats(P, st.dropped, st.flagged, kStatDropped, kStatFlagged);
+    block_stats(P, st.claims, st.rows, kStatClaims, kStatRowReads);
+    block_stats(P, st.fresh, st.captured, kStatFresh, kStatCaptured);
+    block_stats(P, st.rechecks, 0, kStatRechecks, kStatRechecks);
+}
 
 // Growth step of one record with its liquid mask and growth increment loaded. Returns 0: drop
 // the record, 1: keep it unchanged (not eligible yet), 2: keep the updated record.
+// eff_min: the cached minimum critical length, or the second-smallest one once the minimum's
+// neighbour is no longer liquid (both are lower bounds of the current liquid neighbours' lengths).
 __device__ __forceinline__ int grow_record(DomainDesc &D, ActiveRec &r, unsigned int m, double inc, bool inc_ok,
-                                           GrowStats &st) {
+                                           float eff_min, CycleStats &st) {
     const unsigned int c = r.cell;
     st.listed++;
     if (D.done || (m & kMaskDead)) {
-        // finished domain, or solidified by last cycle's re-check
-        D.dl[c] = r.dl;
+        // finished domain, or solidified by last cycle's re-check (a retired domain's records point
+        // at the placeholder descriptor, which has no fields)
+        if (D.dl)
+            D.dl[c] = r.dl;
         return 0;
     }
     if (!(D.cycle > r.cts))
@@ -510,7 +557,7 @@ __device__ __forceinline__ int grow_record(DomainDesc &D, ActiveRec &r, unsigned
         atomicOr(&D.error, kErrGrowthTable);
     const float dl = (float)((double)r.dl + inc);
     r.dl = dl;
-    if ((m & kMaskFresh) || dl >= r.cdl_min) {
+    if ((m & kMaskFresh) || dl >= eff_min) {
         r.cdl_min = __uint_as_float(kNeedsClaim);
         st.flagged++;
         return 2;
@@ -524,14 +571,12 @@ __device__ __forceinline__ int grow_record(DomainDesc &D, ActiveRec &r, unsigned
     return 2;
 }
 
-__device__ __forceinline__ void load_growth(const DomainDesc &D, const ActiveRec &r, unsigned int &m, double &inc,
-                                            bool &ok) {
-    m = D.lmask[r.cell];
-    if (m & kMaskKeep) {
-        // the neighbour verdict of the previous cycle does not carry over
-        m &= ~kMaskKeep;
-        D.lmask[r.cell] = m;
-    }
+__device__ __forceinline__ float effective_min(const ActiveRec &r, unsigned int m, unsigned long long min2) {
+    const unsigned int d1 = (unsigned int)(min2 >> 32);
+    return (d1 >= 26u || ((m >> d1) & 1u)) ? r.cdl_min : __uint_as_float((unsigned int)min2);
+}
+
+__device__ __forceinline__ void load_growth(const DomainDesc &D, const ActiveRec &r, double &inc, bool &ok) {
     // undercooling after the executed updates since the liquidus (src/CAupdate.cpp:236-237)
     long long nu = executed_upto(D, D.cycle) - executed_upto(D, r.cts);
     if (D.zero_du && D.du[r.cell] == 0.0f)
@@ -540,247 +585,357 @@ __device__ __forceinline__ void load_growth(const DomainDesc &D, const ActiveRec
     inc = (ok && D.cycle > r.cts) ? __ldg(D.growth + nu) : 0.0;
 }
 
-__global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
-    const int cur = P->cur;
-    const unsigned long long n = P->cnt[cur];
-    ActiveRec *in = P->rec[cur];
-    const unsigned int *in_dom = P->rdom[cur];
-    DomainDesc *desc = P->desc;
-    GrowStats st;
-    if (!P->compact) {
-        // records are updated in place; dropped ones become tombstones
-        const unsigned long long step = (unsigned long long)gridDim.x * kBlock * kBatch;
-        // block-uniform loop: block_reserve_on is reached by every thread
-        for (unsigned long long b0 = (unsigned long long)blockIdx.x * kBlock * kBatch; b0 < n; b0 += step) {
-            const unsigned long long base = b0 + threadIdx.x;
-            ActiveRec r[kBatch];
-            unsigned int dom[kBatch], m[kBatch];
-            double inc[kBatch];
-            bool ok[kBatch];
+// Records the growth pass hands to the claim pass go to a global queue together with the state the
+// claim pass needs (list position, cell, domain, liquid-neighbour mask, grown DiagonalLength), so the
+// claim pass needs no dependent load before its own round of loads.
+// Warp-aggregated reservation of n slots per lane on a global counter (every lane of the warp
+// calls). Returns this lane's first slot, or ULLONG_MAX past `cap` (the pool error flag is set).
+__device__ __forceinline__ unsigned long long warp_reserve_n(unsigned long long *counter, unsigned long long cap,
+                                                             int *error, unsigned int n) {
+    const unsigned int lane = threadIdx.x & 31;
+    unsigned int incl = n;
 #pragma unroll
-            for (int q = 0; q < kBatch; q++) {
-                const unsigned long long i = base + (unsigned long long)q * kBlock;
-                r[q].cell = kTombstone;
-                dom[q] = 0;
-                if (i < n) {
-                    r[q] = in[i];
-                    dom[q] = in_dom[i];
-                }
-            }
-#pragma unroll
-            for (int q = 0; q < kBatch; q++) {
-                m[q] = 0;
-                inc[q] = 0.0;
-                ok[q] = true;
-                if (r[q].cell != kTombstone)
-                    load_growth(desc[dom[q]], r[q], m[q], inc[q], ok[q]);
-            }
-            unsigned int flagged = 0;
-#pragma unroll
-            for (int q = 0; q < kBatch; q++) {
-                if (r[q].cell == kTombstone)
-                    continue;
-                const unsigned long long i = base + (unsigned long long)q * kBlock;
-                const int a = grow_record(desc[dom[q]], r[q], m[q], inc[q], ok[q], st);
-                if (a == 0) {
-                    ActiveRec tomb = r[q];
-                    tomb.cell = kTombstone;
-                    tomb.cdl_min = 0.0f;
-                    in[i] = tomb;
-                    st.dropped++;
-                }
-                else if (a == 2) {
-                    *reinterpret_cast<float2 *>(&in[i].dl) = make_float2(r[q].dl, r[q].cdl_min);
-                    if (__float_as_uint(r[q].cdl_min) == kNeedsClaim)
-                        flagged |= 1u << q;
-                }
-            }
-            const unsigned long long qpos = block_reserve_on(&P->qcnt, P->capacity, &P->error, __popc(flagged));
-            if (qpos != ULLONG_MAX) {
-                unsigned long long k = qpos;
-#pragma unroll
-                for (int q = 0; q < kBatch; q++)
-                    if (flagged & (1u << q))
-                        P->queue[k++] = (unsigned int)(base + (unsigned long long)q * kBlock);
-            }
-        }
+    for (int o = 1; o < 32; o <<= 1) {
+        unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o)
+            incl += v;
     }
-    else {
-        // compaction: the survivors are written to the other list
-        const int nxt = cur ^ 1;
-        ActiveRec *out = P->rec[nxt];
-        unsigned int *out_dom = P->rdom[nxt];
-        const unsigned long long stride = (unsigned long long)gridDim.x * kBlock;
-        // block-uniform loop: block_reserve is reached by every thread
-        for (unsigned long long i0 = (unsigned long long)blockIdx.x * kBlock; i0 < n; i0 += stride) {
-            const unsigned long long i = i0 + threadIdx.x;
-            bool keep = false;
-            ActiveRec r;
-            unsigned int dom = 0;
-            if (i < n) {
-                r = in[i];
-                dom = in_dom[i];
-                if (r.cell != kTombstone) {
-                    unsigned int m;
-                    double inc;
-                    bool ok;
-                    load_growth(desc[dom], r, m, inc, ok);
-                    keep = grow_record(desc[dom], r, m, inc, ok, st) != 0;
-                }
-            }
-            const unsigned long long pos = block_reserve(P, nxt, keep ? 1u : 0u);
-            const bool flag = keep && pos != ULLONG_MAX && __float_as_uint(r.cdl_min) == kNeedsClaim;
-            if (keep && pos != ULLONG_MAX) {
-                out[pos] = r;
-                out_dom[pos] = dom;
-            }
-            const unsigned long long qpos = block_reserve_on(&P->qcnt, P->capacity, &P->error, flag ? 1u : 0u);
-            if (flag && qpos != ULLONG_MAX)
-                P->queue[qpos] = (unsigned int)pos;
-        }
+    const unsigned int total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned long long base = 0;
+    if (lane == 31 && total)
+        base = atomicAdd(counter, (unsigned long long)total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    if (base + total > cap) {
+        if (lane == 31 && total)
+            atomicOr(error, kErrListOverflow);
+        return ULLONG_MAX;
     }
-    block_stats(P, st.listed, st.grown, kStatListed, kStatGrown);
-    block_stats(P, st.dropped, st.flagged, kStatDropped, kStatFlagged);
-    if (!P->compact) {
-        // dropped records stay as tombstones until the next compaction
-        __shared__ unsigned long long s_d;
-        if (threadIdx.x == 0)
-            s_d = 0;
-        __syncthreads();
-        if (st.dropped)
-            atomicAdd(&s_d, st.dropped);
-        __syncthreads();
-        if (threadIdx.x == 0 && s_d)
-            atomicAdd(&P->tombs, s_d);
-    }
+    return base + incl - n;
 }
 
-__global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
-    const int lst = P->pending; // the list the growth pass just wrote
-    const unsigned long long nq = P->qcnt;
-    ActiveRec *recs = P->rec[lst];
-    const unsigned int *rdom = P->rdom[lst];
-    DomainDesc *desc = P->desc;
-    unsigned long long st_claims = 0, st_rows = 0, st_fresh = 0, st_dropped = 0;
-    const unsigned long long nthreads = (unsigned long long)gridDim.x * kBlock;
-    const unsigned long long me = (unsigned long long)threadIdx.x * gridDim.x + blockIdx.x;
-    // block-uniform loop (block_reserve_on); consecutive items on different blocks
-    for (unsigned long long q0 = 0; q0 < nq; q0 += nthreads) {
-        const unsigned long long qi = q0 + me;
-        unsigned int first = 0, pushed_dom = 0;
-        unsigned int pushed_cell = 0;
-        int first_plane = 0, first_my = 0;
-        do {
-        if (qi >= nq)
-            break;
-        const unsigned long long i = P->queue[qi];
-        const ActiveRec rec = recs[i];
-        if (rec.cell == kTombstone || __float_as_uint(rec.cdl_min) != kNeedsClaim)
-            continue;
-        const unsigned int c = rec.cell;
-        const unsigned int dom = rdom[i];
-        DomainDesc &D = desc[dom];
-        const float dl = rec.dl;
-        const int plane = D.mx * D.my, my = D.my;
+// Claim work of queue entry k. Returns the directions of the cells it claimed. All loads of the entry
+// (critical-length row, neighbour types) go out in one round.
+__device__ __forceinline__ unsigned int claim_entry(PoolState *P, ActiveRec *recs, unsigned long long k,
+                                                    CycleStats &st, unsigned long long &tombs) {
+    const unsigned int i = __ldcg(P->qpos + k), c = __ldcg(P->qcell + k), dom = __ldcg(P->qdom + k);
+    unsigned int m = __ldcg(P->qmask + k);
+    const float dl = __ldcg(P->qdl + k);
+    DomainDesc &D = P->desc[dom];
+    const int plane = D.mx * D.my, my = D.my;
+    // the 26 critical lengths as 13 aligned 8-byte loads (26 * 4 * c is 8-byte aligned)
+    const float2 *row = reinterpret_cast<const float2 *>(D.cdl + 26ull * c);
+    float cdl[26];
+#pragma unroll
+    for (int q = 0; q < 13; q++) {
+        const float2 v = __ldcg(row + q);
+        cdl[2 * q] = v.x;
+        cdl[2 * q + 1] = v.y;
+    }
+    if (m & kMaskFresh) {
+        // liquid neighbours from the 26 neighbour types (src/CAupdate.cpp:320-334); no other thread
+        // writes this cell's mask now, captures and nucleations clear bits later. Invalid directions
+        // read the cell itself.
+        st.fresh++;
         int rx, ry, rz;
         cell_coords(D, c, rx, ry, rz);
-        unsigned int m = D.lmask[c];
-        if (m & kMaskFresh) {
-            // liquid neighbours from the 26 neighbour types (src/CAupdate.cpp:320-334); no other
-            // thread writes this cell's mask now, captures and nucleations clear bits later
-            st_fresh++;
-            const unsigned int valid = neighbour_mask(D, rx, ry, rz);
-            const int8_t *ct = D.ctype + c;
-            m = 0;
-#pragma unroll
-            for (int l = 0; l < 26; l++)
-                if ((valid & (1u << l)) && ct[nb_offset(l, plane, my)] == kLiquid)
-                    m |= 1u << l;
-            D.lmask[c] = m;
-        }
-        if (m == 0) {
-            // no liquid neighbour: LCount stays 0 (src/CAupdate.cpp:722-725)
-            D.ctype[c] = kSolid;
-            D.dl[c] = dl;
-            ActiveRec tomb = rec;
-            tomb.cell = kTombstone;
-            tomb.cdl_min = 0.0f;
-            recs[i] = tomb;
-            st_dropped++;
-            continue;
-        }
-        // the 26 critical lengths as 13 aligned 8-byte loads (26 * 4 * c is 8-byte aligned)
-        st_rows++;
-        const float2 *row = reinterpret_cast<const float2 *>(D.cdl + 26ull * c);
-        float cdl[26];
-#pragma unroll
-        for (int q = 0; q < 13; q++) {
-            float2 v = row[q];
-            cdl[2 * q] = v.x;
-            cdl[2 * q + 1] = v.y;
-        }
-        float nm = __int_as_float(0x7f800000);
-        unsigned int reach = 0;
+        const unsigned int valid = neighbour_mask(D, rx, ry, rz);
+        const int8_t *ct = D.ctype + c;
+        m = 0;
 #pragma unroll
         for (int l = 0; l < 26; l++) {
-            if (m & (1u << l)) {
-                nm = (cdl[l] < nm) ? cdl[l] : nm;
-                if (dl >= cdl[l])
-                    reach |= 1u << l;
-            }
+            const bool v = (valid >> l) & 1u;
+            const int8_t nt = __ldcg(ct + (v ? nb_offset(l, plane, my) : 0));
+            m |= (v && nt == kLiquid) ? (1u << l) : 0u;
         }
-        recs[i].cdl_min = nm;
-        if (reach) {
-            // claims (src/CAupdate.cpp:336-352): lowest index wins; the first claimant of a cell in
-            // this cycle lists it for k_capture / k_neighbours
-            const unsigned long long key = ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
-            const unsigned int want = 0xffffffffu - D.epoch;
+        P->rstat[P->pending][i] = m;
+    }
+    if (m == 0) {
+        // no liquid neighbour: LCount stays 0 (src/CAupdate.cpp:722-725)
+        D.ctype[c] = kSolid;
+        D.dl[c] = dl;
+        recs[i].cell = kTombstone;
+        recs[i].cdl_min = 0.0f;
+        st.dropped++;
+        tombs++;
+        return 0;
+    }
+    st.rows++;
+    // Every reached cell is claimed and captured within this cycle, so the cached minimum only
+    // covers the liquid neighbours not reached (+inf when none is left).
+    float nm = __int_as_float(0x7f800000), nm2 = nm;
+    unsigned int d1 = 0xffffffffu;
+    unsigned int reach = 0;
 #pragma unroll
-            for (int l = 0; l < 26; l++) {
-                if (reach & (1u << l)) {
-                    unsigned long long old = atomicMin(D.claim + (long long)c + nb_offset(l, plane, my), key);
-                    if ((unsigned int)(old >> 32) != want)
-                        first |= 1u << l;
-                }
+    for (int l = 0; l < 26; l++) {
+        if (m & (1u << l)) {
+            if (dl >= cdl[l]) {
+                reach |= 1u << l;
             }
-            st_claims += __popc(reach);
-            pushed_dom = dom;
-            pushed_cell = c;
-            first_plane = plane;
-            first_my = my;
-        }
-        } while (false);
-        // list the cells this thread claimed first (block-aggregated reservation)
-        const unsigned long long pos = block_reserve_on(&P->tcnt, P->capacity, &P->error, __popc(first));
-        if (pos != ULLONG_MAX) {
-            unsigned long long k = pos;
-            for (unsigned int bits = first; bits; bits &= bits - 1) {
-                int l = __ffs(bits) - 1;
-                P->tgt[k++] = ((unsigned long long)pushed_dom << 32) |
-                              (unsigned int)((long long)pushed_cell + nb_offset(l, first_plane, first_my));
+            else if (cdl[l] < nm) {
+                nm2 = nm;
+                nm = cdl[l];
+                d1 = l;
+            }
+            else if (cdl[l] < nm2) {
+                nm2 = cdl[l];
             }
         }
     }
-    block_stats(P, st_claims, st_rows, kStatClaims, kStatRowReads);
-    block_stats(P, st_fresh, 0, kStatFresh, kStatFresh);
-    if (st_dropped && !P->compact)
-        atomicAdd(&P->tombs, st_dropped);
+    recs[i].cdl_min = nm;
+    P->rmin2[P->pending][i] = ((unsigned long long)d1 << 32) | __float_as_uint(nm2);
+    if (reach) {
+        // claims (src/CAupdate.cpp:336-352): the lowest index wins. Nothing waits for them: every
+        // claimant lists its claim and the capture pass keeps the winner's.
+        const unsigned long long key = ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
+        unsigned long long *base = D.claim + c;
+        for (unsigned int bits = reach; bits; bits &= bits - 1)
+            atomicMin(base + nb_offset(__ffs(bits) - 1, plane, my), key);
+        st.claims += __popc(reach);
+    }
+    return reach;
 }
 
-// Every cell claimed this cycle is captured by its lowest-index claimant (src/CAupdate.cpp:336-563,
-// 713-717). Two independent passes over the claimed cells:
-//   k_capture     one thread per claimed cell: the new octahedron, 26 critical lengths, GrainID,
-//                 and its record in the next cycle's list.
-//   k_neighbours  26 threads per claimed cell: each active neighbour drops the cell from its liquid
-//                 mask, and a neighbour grown this cycle re-checks whether it still sees a liquid
-//                 cell (src/CAupdate.cpp:722-725). With kTail the last block to finish starts the
-//                 next cycle.
-// Neither pass reads what the other writes: the re-check uses the claims and the unclaimed mask
-// bits only, and a cell being captured still has its initial (not yet built) mask.
-__global__ void __launch_bounds__(kBlock) k_capture(PoolState *P) {
+// Puts the flagged records of one growth step into the claim queue (all lanes of the warp call).
+__device__ __forceinline__ void queue_flagged(PoolState *P, unsigned int shard, unsigned int nf, unsigned int flagged,
+                                              const unsigned long long *idx, const ActiveRec *r,
+                                              const unsigned int *dom, const unsigned int *m) {
+    unsigned long long k = warp_reserve_n(&P->qcnt_s[shard].v, P->shard_cap, &P->error, nf);
+    if (nf && k != ULLONG_MAX) {
+        k += (unsigned long long)shard * P->shard_cap;
+#pragma unroll
+        for (int q = 0; q < kBatch; q++) {
+            if (flagged & (1u << q)) {
+                P->qpos[k] = (unsigned int)idx[q];
+                P->qcell[k] = r[q].cell;
+                P->qdom[k] = dom[q];
+                P->qmask[k] = m[q];
+                P->qdl[k] = r[q].dl;
+                k++;
+            }
+        }
+    }
+}
+
+// Growth step of a compaction cycle: the survivors are written to the other list (rare; kept out of
+// line).
+__device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long long gw, unsigned long long nw,
+                                         unsigned long long n, CycleStats &st) {
+    const unsigned int lane = threadIdx.x & 31;
+    DomainDesc *desc = P->desc;
+    const ActiveRec *in = P->rec[cur];
+    const unsigned int *in_dom = P->rdom[cur];
+    const unsigned int *in_stat = P->rstat[cur];
+    const unsigned long long *in_min2 = P->rmin2[cur];
+    const int nxt = cur ^ 1;
+    ActiveRec *out = P->rec[nxt];
+    unsigned int *out_dom = P->rdom[nxt];
+    unsigned int *out_stat = P->rstat[nxt];
+    unsigned long long *out_min2 = P->rmin2[nxt];
+    const unsigned long long groups = (n + 31) / 32;
+    for (unsigned long long g = gw; g < groups; g += nw) {
+        unsigned long long i = g * 32 + lane;
+        bool keep = false;
+        ActiveRec r;
+        r.cell = kTombstone;
+        unsigned int dom = 0, m = 0;
+        unsigned long long mn2 = kNoMin2;
+        if (i < n) {
+            const int4 v = __ldcg(reinterpret_cast<const int4 *>(in + i));
+            r = *reinterpret_cast<const ActiveRec *>(&v);
+            dom = __ldcg(in_dom + i);
+            m = __ldcg(in_stat + i) & ~kMaskKeep;
+            mn2 = __ldcg(in_min2 + i);
+            if (r.cell != kTombstone) {
+                double inc;
+                bool ok;
+                load_growth(desc[dom], r, inc, ok);
+                keep = grow_record(desc[dom], r, m, inc, ok, effective_min(r, m, mn2), st) != 0;
+                if (!keep)
+                    st.dropped++;
+            }
+        }
+        const unsigned long long pos = warp_reserve_n(&P->cnt[nxt], P->capacity, &P->error, keep ? 1u : 0u);
+        const bool placed = keep && pos != ULLONG_MAX;
+        if (placed) {
+            out[pos] = r;
+            out_dom[pos] = dom;
+            out_stat[pos] = m;
+            out_min2[pos] = mn2;
+            desc[dom].pos[r.cell] = (unsigned int)pos;
+        }
+        const bool flag = placed && __float_as_uint(r.cdl_min) == kNeedsClaim;
+        unsigned long long idx = pos;
+        queue_flagged(P, (unsigned int)(gw % kShards), flag ? 1u : 0u, flag ? 1u : 0u, &idx, &r, &dom, &m);
+    }
+}
+
+// Active records are handed out to warps in groups of 32 consecutive records (one coalesced load),
+// group g to warp g % (number of warps of the grid), consecutive warps on different blocks: the
+// records appended by the last capture pass, which all need a fresh mask and claims, spread over
+// every SM. No block-wide synchronisation.
+__device__ void grow_pass(PoolState *P, CycleStats &st) {
+    const int cur = P->cur;
+    const unsigned long long n = P->cnt[cur];
+    const unsigned int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned long long nw = (unsigned long long)gridDim.x * (kBlock / 32);
+    const unsigned long long gw = (unsigned long long)warp * gridDim.x + blockIdx.x;
+    if (P->compact) {
+        compact_pass(P, cur, gw, nw, n, st);
+        return;
+    }
+    ActiveRec *in = P->rec[cur];
+    const unsigned int *in_dom = P->rdom[cur];
+    unsigned int *in_stat = P->rstat[cur];
+    const unsigned long long *in_min2 = P->rmin2[cur];
+    DomainDesc *desc = P->desc;
+    unsigned long long tombs = 0;
+    const unsigned long long groups = (n + 31) / 32;
+    // records are updated in place; dropped ones become tombstones
+    for (unsigned long long g0 = gw; g0 < groups; g0 += kBatch * nw) {
+        ActiveRec r[kBatch];
+        unsigned int dom[kBatch], m[kBatch];
+        unsigned long long idx[kBatch], mn2[kBatch];
+        double inc[kBatch];
+        bool ok[kBatch];
+#pragma unroll
+        for (int q = 0; q < kBatch; q++) {
+            idx[q] = (g0 + (unsigned long long)q * nw) * 32 + lane;
+            r[q].cell = kTombstone;
+            dom[q] = 0;
+            m[q] = 0;
+            mn2[q] = kNoMin2;
+            if (idx[q] < n) {
+                // streamed once per cycle: through L2 only
+                const int4 v = __ldcg(reinterpret_cast<const int4 *>(in + idx[q]));
+                r[q] = *reinterpret_cast<const ActiveRec *>(&v);
+                dom[q] = __ldcg(in_dom + idx[q]);
+                m[q] = __ldcg(in_stat + idx[q]);
+                mn2[q] = __ldcg(in_min2 + idx[q]);
+            }
+        }
+#pragma unroll
+        for (int q = 0; q < kBatch; q++) {
+            inc[q] = 0.0;
+            ok[q] = true;
+            if (r[q].cell != kTombstone) {
+                if (m[q] & kMaskKeep) {
+                    // the neighbour verdict of the previous cycle does not carry over
+                    m[q] &= ~kMaskKeep;
+                    in_stat[idx[q]] = m[q];
+                }
+                load_growth(desc[dom[q]], r[q], inc[q], ok[q]);
+            }
+        }
+        unsigned int flagged = 0;
+#pragma unroll
+        for (int q = 0; q < kBatch; q++) {
+            if (r[q].cell == kTombstone)
+                continue;
+            const int a = grow_record(desc[dom[q]], r[q], m[q], inc[q], ok[q], effective_min(r[q], m[q], mn2[q]), st);
+            if (a == 0) {
+                in[idx[q]].cell = kTombstone;
+                in[idx[q]].cdl_min = 0.0f;
+                st.dropped++;
+                tombs++;
+            }
+            else if (a == 2) {
+                *reinterpret_cast<float2 *>(&in[idx[q]].dl) = make_float2(r[q].dl, r[q].cdl_min);
+                if (__float_as_uint(r[q].cdl_min) == kNeedsClaim)
+                    flagged |= 1u << q;
+            }
+        }
+        queue_flagged(P, (unsigned int)(gw % kShards), __popc(flagged), flagged, idx, r, dom, m);
+    }
+    // dropped records stay as tombstones of the in-place list until the next compaction
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+        tombs += __shfl_down_sync(0xffffffffu, tombs, o);
+    if (lane == 0 && tombs)
+        atomicAdd(&P->tomb_s[gw % kShards].v, tombs);
+}
+
+// Exclusive prefix of the shard counts in shared memory (all threads of the block call).
+__device__ __forceinline__ void shard_prefix(const ShardCounter *cnt, unsigned long long *pre) {
+    if (threadIdx.x < 32) {
+        const unsigned int lane = threadIdx.x;
+        const unsigned long long c = __ldcg(&cnt[lane].v);
+        unsigned long long incl = c;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            unsigned long long v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (unsigned)o)
+                incl += v;
+        }
+        pre[lane + 1] = incl;
+        if (lane == 0)
+            pre[0] = 0;
+    }
+    __syncthreads();
+}
+
+// Position in the sharded array of the k-th entry of the shards' concatenation.
+__device__ __forceinline__ unsigned long long shard_entry(const unsigned long long *pre, unsigned long long cap,
+                                                          unsigned long long k) {
+    int lo = 0;
+#pragma unroll
+    for (int step = 16; step; step >>= 1)
+        if (pre[lo + step] <= k)
+            lo += step;
+    return (unsigned long long)lo * cap + (k - pre[lo]);
+}
+
+// One queue entry per thread, consecutive warps on different blocks; every claim is listed.
+__device__ void claim_pass(PoolState *P, CycleStats &st) {
+    __shared__ unsigned long long s_pre[kShards + 1];
+    shard_prefix(P->qcnt_s, s_pre);
+    const unsigned long long nq = s_pre[kShards];
+    const unsigned long long cap = P->shard_cap;
+    ActiveRec *recs = P->rec[P->pending];
+    const unsigned int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const unsigned long long nw = (unsigned long long)gridDim.x * (kBlock / 32);
+    const unsigned long long gw = (unsigned long long)warp * gridDim.x + blockIdx.x;
+    unsigned long long tombs = 0;
+    for (unsigned long long k0 = gw * 32; k0 < nq; k0 += nw * 32) {
+        const unsigned long long k = k0 + lane;
+        unsigned int reach = 0, dom = 0, cell = 0;
+        if (k < nq) {
+            const unsigned long long e = shard_entry(s_pre, cap, k);
+            reach = claim_entry(P, recs, e, st, tombs);
+            dom = __ldcg(P->qdom + e);
+            cell = __ldcg(P->qcell + e);
+        }
+        const unsigned int ts = (unsigned int)(gw % kShards);
+        unsigned long long pos = warp_reserve_n(&P->tcnt_s[ts].v, cap, &P->error, __popc(reach));
+        if (reach && pos != ULLONG_MAX) {
+            pos += (unsigned long long)ts * cap;
+            const DomainDesc &D = P->desc[dom];
+            const int plane = D.mx * D.my, my = D.my;
+            unsigned long long t = pos;
+            for (unsigned int bits = reach; bits; bits &= bits - 1) {
+                const int l = __ffs(bits) - 1;
+                P->tgt[t++] = ((unsigned long long)dom << 37) | ((unsigned long long)l << 32) |
+                              (unsigned int)((long long)cell + nb_offset(l, plane, my));
+            }
+        }
+    }
+    if (!P->compact) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1)
+            tombs += __shfl_down_sync(0xffffffffu, tombs, o);
+        if (lane == 0 && tombs)
+            atomicAdd(&P->tomb_s[gw % kShards].v, tombs);
+    }
+}
+
+__device__ void capture_pass(PoolState *P, CycleStats &st) {
+    __shared__ unsigned long long s_pre[kShards + 1];
+    shard_prefix(P->tcnt_s, s_pre);
     const int app = P->pending; // list of the next cycle
-    const unsigned long long T = P->tcnt;
-    // claimed cell j gets record slot base + j (the count grows by T in k_neighbours)
+    const unsigned long long T = s_pre[kShards];
+    const unsigned long long cap = P->shard_cap;
+    // records of the cells active at the start of the cycle lie below base; claim j of the cycle
+    // gets record slot base + j (a tombstone unless it won), and the count grows by T when the
+    // cycle finishes
     const unsigned long long base = P->cnt[app];
     if (base + T > P->capacity) {
         if (threadIdx.x == 0 && blockIdx.x == 0)
@@ -788,26 +943,79 @@ __global__ void __launch_bounds__(kBlock) k_capture(PoolState *P) {
         return;
     }
     DomainDesc *desc = P->desc;
+    unsigned long long losers = 0;
+    unsigned int *rs = P->rstat[app];
+    constexpr int kGroups = 32 / kCaptureLanes;
+    constexpr int kPer = (26 + kCaptureLanes - 1) / kCaptureLanes;
     const int lane = threadIdx.x & 31;
-    // one warp per claimed cell, consecutive cells on different blocks (spread over all SMs)
-    const unsigned long long nwarps = (unsigned long long)gridDim.x * (kBlock / 32);
-    const unsigned long long w0 = (unsigned long long)(threadIdx.x >> 5) * gridDim.x + blockIdx.x;
-    unsigned long long st_cap = 0;
-    for (unsigned long long j = w0; j < T; j += nwarps) {
-        const unsigned long long e = P->tgt[j];
-        const unsigned int dom = (unsigned int)(e >> 32);
+    const int grp = lane / kCaptureLanes, sub = lane % kCaptureLanes;
+    // consecutive claims on different blocks (spread over all SMs)
+    const unsigned long long ngroups = (unsigned long long)gridDim.x * (kBlock / 32) * kGroups;
+    const unsigned long long g0 = ((unsigned long long)(threadIdx.x >> 5) * gridDim.x + blockIdx.x) * kGroups + grp;
+    for (unsigned long long j = g0; j < T; j += ngroups) {
+        const unsigned long long e = __ldcg(P->tgt + shard_entry(s_pre, cap, j));
         const unsigned int t = (unsigned int)e;
+        const int l = (int)((e >> 32) & 31u);
+        const unsigned int dom = (unsigned int)(e >> 37);
         DomainDesc &D = desc[dom];
-        const unsigned int w = (unsigned int)__ldcg(D.claim + t);
+        const int plane = D.mx * D.my, my = D.my;
+        const unsigned int c = (unsigned int)((long long)t - nb_offset(l, plane, my)); // the claimant
+        // Every load of the capture and of the re-checks goes out in one round; only the group of
+        // the winning claim (the lowest claimant index) continues.
+        const unsigned long long key = __ldcg(D.claim + t);
         const int cts_t = __ldg(D.cts + t);
-        int wx, wy, wz, tx, ty, tz;
-        cell_coords(D, w, wx, wy, wz);
+        const int h = __ldcg(D.gid + c);
+        const float docx = __ldcg(D.doc + 3ull * c + 0), docy = __ldcg(D.doc + 3ull * c + 1),
+                    docz = __ldcg(D.doc + 3ull * c + 2);
+        int tx, ty, tz;
         cell_coords(D, t, tx, ty, tz);
-        const int l = c_dir[(tz - wz + 1) * 9 + (tx - wx + 1) * 3 + (ty - wy + 1)];
-        const float new_dl = capture_cell(D, w, t, l, lane);
-        __syncwarp();
-        if (lane == 0) {
-            D.lmask[t] = kMaskFresh;
+        const unsigned int valid = neighbour_mask(D, tx, ty, tz);
+        unsigned int a[kPer], p[kPer], old[kPer];
+        int8_t ct[kPer];
+        int cts_a[kPer];
+        bool act[kPer];
+#pragma unroll
+        for (int k = 0; k < kPer; k++) {
+            const int ln = sub + k * kCaptureLanes;
+            act[k] = ln < 26 && (valid & (1u << ln));
+            a[k] = (unsigned int)((long long)t + (act[k] ? nb_offset(ln, plane, my) : 0));
+            ct[k] = __ldcg(D.ctype + a[k]);
+            p[k] = __ldcg(D.pos + a[k]);
+            cts_a[k] = __ldg(D.cts + a[k]);
+        }
+        if ((unsigned int)key != c) {
+            // a lower-index claimant captures t; this claim's slot stays a dropped record
+            if (sub == 0) {
+                P->rec[app][base + j].cell = kTombstone;
+                P->rec[app][base + j].cdl_min = 0.0f;
+                losers++;
+            }
+            continue;
+        }
+        const unsigned int w = c;
+        // Serial order (src/CAupdate.cpp:333-334, 722-725): active cell a saw the captured cell t
+        // as liquid iff t's capturer w does not precede a. a keeps a liquid neighbour iff it has an
+        // unclaimed one (a set mask bit that nobody clears) or a claimed one with w >= a. Every
+        // claimed liquid neighbour clears its own bit exactly once, so the update that clears the
+        // last direction bit sees the final verdict: KEEP is always set before the clear of the
+        // same update, and an update's two atomics reach the word in program order. Only records of
+        // cells active at the start of the cycle (positions below base) take part: a neighbour
+        // captured in this same cycle reads as liquid, or has no record below base.
+#pragma unroll
+        for (int k = 0; k < kPer; k++)
+            act[k] = act[k] && ct[k] == kActive && p[k] < base;
+#pragma unroll
+        for (int k = 0; k < kPer; k++)
+            if (act[k] && w >= a[k])
+                atomicOr(rs + p[k], kMaskKeep);
+#pragma unroll
+        for (int k = 0; k < kPer; k++) {
+            old[k] = 0;
+            if (act[k])
+                old[k] = atomicAnd(rs + p[k], ~(1u << c_opp[sub + k * kCaptureLanes]));
+        }
+        const float new_dl = capture_cell<kCaptureLanes>(D, c, t, l, sub, h, docx, docy, docz);
+        if (sub == 0) {
             ActiveRec r;
             r.cell = t;
             r.dl = new_dl;
@@ -815,79 +1023,188 @@ __global__ void __launch_bounds__(kBlock) k_capture(PoolState *P) {
             r.cts = cts_t;
             P->rec[app][base + j] = r;
             P->rdom[app][base + j] = dom;
-            // read as active only from the next kernel on, after the octahedron data is written
+            rs[base + j] = kMaskFresh;
+            P->rmin2[app][base + j] = kNoMin2;
+            D.pos[t] = (unsigned int)(base + j);
+            // read as active by the growth pass of the next cycle, after the octahedron is written
             D.ctype[t] = kActive;
             atomicAdd((unsigned long long *)&D.liquid_shard[(blockIdx.x + j) & (kLiquidShards - 1)],
                       (unsigned long long)(-1ll));
-            st_cap++;
+            st.captured++;
+        }
+#pragma unroll
+        for (int k = 0; k < kPer; k++) {
+            if (!act[k])
+                continue;
+            const unsigned int bit = 1u << c_opp[sub + k * kCaptureLanes];
+            if ((old[k] & (kMaskFresh | kMaskDead)) || (old[k] & kDirBits) != bit || (old[k] & kMaskKeep))
+                continue;
+            // a lost its last liquid neighbour; it solidifies if it was grown this cycle
+            if (D.cycle > cts_a[k]) {
+                st.rechecks++;
+                D.ctype[a[k]] = kSolid;
+                atomicOr(rs + p[k], kMaskDead);
+            }
         }
     }
-    block_stats(P, st_cap, 0, kStatCaptured, kStatCaptured);
+    // every lane reaches this point
+#pragma unroll
+    for (int o = 16; o; o >>= 1)
+        losers += __shfl_down_sync(0xffffffffu, losers, o);
+    if (lane == 0 && losers)
+        atomicAdd(&P->tomb_s[(blockIdx.x + threadIdx.x) % kShards].v, losers);
 }
 
-template <bool kTail> __global__ void __launch_bounds__(kBlock) k_neighbours(PoolState *P) {
-    const unsigned long long n = P->tcnt * 26ull;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        // the records k_capture wrote at fixed slots join the next cycle's list
-        const int app = P->pending;
-        if (P->cnt[app] + P->tcnt <= P->capacity)
-            P->cnt[app] += P->tcnt;
-    }
-    DomainDesc *desc = P->desc;
-    unsigned long long st_rc = 0;
-    // consecutive items on different blocks (spread over all SMs)
-    const unsigned long long nthreads = (unsigned long long)gridDim.x * kBlock;
-    for (unsigned long long j = (unsigned long long)threadIdx.x * gridDim.x + blockIdx.x; j < n; j += nthreads) {
-        const unsigned long long q = j / 26ull;
-        const int l = (int)(j - q * 26ull);
-        const unsigned long long e = P->tgt[q];
-        const unsigned int dom = (unsigned int)(e >> 32);
-        const unsigned int t = (unsigned int)e;
-        DomainDesc &D = desc[dom];
-        int tx, ty, tz;
-        cell_coords(D, t, tx, ty, tz);
-        if (!(neighbour_mask(D, tx, ty, tz) & (1u << l)))
-            continue;
-        const unsigned int a = (unsigned int)((long long)t + nb_offset(l, D.mx * D.my, D.my));
-        const unsigned int w = (unsigned int)__ldcg(D.claim + t);
-        if (__ldcg(D.ctype + a) != kActive)
-            continue;
-        // Serial order (src/CAupdate.cpp:333-334, 722-725): active cell a saw the captured cell t
-        // as liquid iff t's capturer w does not precede a. a keeps a liquid neighbour iff it has an
-        // unclaimed one (a set mask bit that nobody clears) or a claimed one with w >= a. Every
-        // claimed liquid neighbour clears its own bit exactly once, so the update that clears the
-        // last direction bit sees the final verdict: KEEP is always set before the clear of the
-        // same update, and an update's two atomics reach the word in program order.
-        if (w >= a)
-            atomicOr(D.lmask + a, kMaskKeep);
-        const unsigned int bit = 1u << c_opp[l];
-        const unsigned int old = atomicAnd(D.lmask + a, ~bit);
-        if ((old & (kMaskFresh | kMaskDead)) || (old & kDirBits) != bit || (old & kMaskKeep))
-            continue;
-        // a lost its last liquid neighbour; it solidifies if it was grown this cycle
-        if (D.cycle > __ldg(D.cts + a)) {
-            st_rc++;
-            D.ctype[a] = kSolid;
-            atomicOr(D.lmask + a, kMaskDead);
+// End of a cycle: the record slots of this cycle's claims join the list.
+__device__ void finish_capture(PoolState *P) {
+    if (threadIdx.x < 32) {
+        unsigned long long T = __ldcg(&P->tcnt_s[threadIdx.x].v);
+#pragma unroll
+        for (int o = 16; o; o >>= 1)
+            T += __shfl_down_sync(0xffffffffu, T, o);
+        if (threadIdx.x == 0) {
+            const int app = P->pending;
+            if (P->cnt[app] + T <= P->capacity)
+                P->cnt[app] += T;
         }
     }
-    block_stats(P, st_rc, 0, kStatRechecks, kStatRechecks);
-    if (kTail) {
-        __shared__ int s_last;
-        __threadfence(); // this block's writes are visible device-wide before it is counted
+    __syncthreads();
+}
+
+__global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
+    CycleStats st;
+    grow_pass(P, st);
+    flush_stats(P, st);
+}
+
+__global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
+    CycleStats st;
+    claim_pass(P, st);
+    flush_stats(P, st);
+}
+
+// Capture pass as its own kernel; the last block to finish closes the cycle and, with kBegin,
+// starts the next one.
+template <bool kBegin> __global__ void __launch_bounds__(kBlock) k_capture_pass(PoolState *P) {
+    CycleStats st;
+    capture_pass(P, st);
+    flush_stats(P, st);
+    __shared__ int s_last;
+    __threadfence(); // this block's writes are visible device-wide before it is counted
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned int prev = atomicAdd(&P->blocks_done, 1u);
+        s_last = (prev == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        if (threadIdx.x == 0)
+            P->blocks_done = 0;
+        finish_capture(P);
+        if (kBegin)
+            begin_cycle(P);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Grid-wide meeting point of the persistent kernel (all blocks co-resident: cooperative launch).
+// Arrival is an acq_rel atomic on a counter, release an st.release of the next generation; the
+// last block to arrive runs `serial` with the whole block before it releases the others. Every
+// wait is bounded: after kMeetTimeoutNs (or kMeetSpinCap polls) the block sets kErrBarrier and
+// the kernel ends.
+constexpr unsigned long long kMeetTimeoutNs = 1000000000ull;
+constexpr unsigned int kMeetSpinCap = 1u << 26;
+
+__device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
+    unsigned int v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ unsigned int atom_add_acq_rel_u32(unsigned int *p, unsigned int v) {
+    unsigned int old;
+    asm volatile("atom.acq_rel.gpu.global.add.u32 %0, [%1], %2;" : "=r"(old) : "l"(p), "r"(v) : "memory");
+    return old;
+}
+__device__ __forceinline__ void st_release_u32(unsigned int *p, unsigned int v) {
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// With P->timeline set, meeting point `tag` records its first arrival, last arrival and release.
+template <class F> __device__ bool grid_meet(PoolState *P, int tag, F &&serial) {
+    __shared__ unsigned int s_gen;
+    __shared__ int s_state; // 0: released, 1: last to arrive, 2: gave up waiting
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned int gen = ld_acquire_u32(&P->bar_gen);
+        const unsigned int prev = atom_add_acq_rel_u32(&P->bar_count, 1u);
+        unsigned long long *tl = P->timeline;
+        if (tl && prev == 0)
+            tl[3 * tag + 0] = global_ns();
+        int state = 0;
+        if (prev == gridDim.x - 1) {
+            state = 1;
+            if (tl)
+                tl[3 * tag + 1] = global_ns();
+        }
+        else {
+            const unsigned long long t0 = global_ns();
+            unsigned int it = 0;
+            while (ld_acquire_u32(&P->bar_gen) == gen) {
+                ++it;
+                if (it >= kMeetSpinCap || ((it & 255u) == 0 && global_ns() - t0 > kMeetTimeoutNs)) {
+                    atomicOr(&P->error, kErrBarrier);
+                    state = 2;
+                    break;
+                }
+                __nanosleep(32);
+            }
+        }
+        s_gen = gen;
+        s_state = state;
+    }
+    __syncthreads();
+    const int state = s_state;
+    if (state == 1) {
+        serial();
         __syncthreads();
         if (threadIdx.x == 0) {
-            unsigned int prev = atomicAdd(&P->blocks_done, 1u);
-            s_last = (prev == gridDim.x - 1);
-        }
-        __syncthreads();
-        if (s_last) {
-            __threadfence();
-            if (threadIdx.x == 0)
-                P->blocks_done = 0;
-            begin_cycle(P);
+            if (P->timeline)
+                P->timeline[3 * tag + 2] = global_ns();
+            P->bar_count = 0;
+            st_release_u32(&P->bar_gen, s_gen + 1u);
         }
     }
+    return state != 2;
+}
+
+// n_cycles complete CA cycles (start, grow/claim, capture) in one cooperative launch.
+__global__ void __launch_bounds__(kBlock, 2) k_cycles(PoolState *P, int n_cycles) {
+    CycleStats st;
+    bool ok = grid_meet(P, 0, [&] { begin_cycle(P); });
+    for (int c = 0; ok && c < n_cycles; c++) {
+        grow_pass(P, st);
+        ok = grid_meet(P, 3 * c + 1, [] {});
+        if (!ok)
+            break;
+        claim_pass(P, st);
+        ok = grid_meet(P, 3 * c + 2, [] {});
+        if (!ok)
+            break;
+        capture_pass(P, st);
+        const bool more = c + 1 < n_cycles;
+        ok = grid_meet(P, 3 * c + 3, [&] {
+            finish_capture(P);
+            if (more)
+                begin_cycle(P);
+        });
+    }
+    flush_stats(P, st);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -999,6 +1316,9 @@ __global__ void k_init_active(PoolState *P, int dom, int list_slot) {
             r.cts = D.cts[c];
             P->rec[list_slot][pos] = r;
             P->rdom[list_slot][pos] = (unsigned int)dom;
+            P->rstat[list_slot][pos] = kMaskFresh;
+            P->rmin2[list_slot][pos] = kNoMin2;
+            D.pos[c] = (unsigned int)pos;
         }
     }
 }
@@ -1022,8 +1342,10 @@ __global__ void k_flush_records(PoolState *P) {
     for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
          i += (unsigned long long)gridDim.x * blockDim.x) {
         const ActiveRec r = P->rec[nxt][i];
+        if (r.cell == kTombstone)
+            continue; // a dropped record's other fields are not kept up to date
         const DomainDesc &D = P->desc[P->rdom[nxt][i]];
-        if (r.cell != kTombstone && D.dl)
+        if (D.dl)
             D.dl[r.cell] = r.dl;
     }
 }
@@ -1115,7 +1437,27 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
     CUDA_OK(cudaMemcpyToSymbol(c_zplus, &zplus, sizeof(zplus)));
     CUDA_OK(cudaMemcpyToSymbol(c_zminus, &zminus, sizeof(zminus)));
     max_domains_ = 8192;
+    // list positions are 32-bit in the passes' block-local queues
+    if (list_capacity > 0xffffffffull)
+        throw Unsupported("list capacity above 2^32 - 1 records");
     capacity_ = std::max<unsigned long long>(list_capacity, 1024);
+    int coop = 0;
+    CUDA_OK(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, device));
+    if (!coop)
+        throw DeviceError("device does not support cooperative launches");
+    int b = 0;
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cycles, kBlock, 0));
+    if (b < 1)
+        throw DeviceError("persistent kernel does not fit on an SM");
+    grid_cycles_ = num_sms_ * b;
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_grow, kBlock, 0));
+    grid_grow_ = num_sms_ * std::max(b, 1);
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_claim, kBlock, 0));
+    grid_claim_ = num_sms_ * std::max(b, 1);
+    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_capture_pass<false>, kBlock, 0));
+    grid_capture_ = num_sms_ * std::max(b, 1);
+    if (const char *m = std::getenv("EXACA_STEP_MODE"))
+        step_mode_ = std::string(m) == "graph" ? 1 : 0;
     CUDA_OK(cudaMalloc(&dstate_, sizeof(PoolState)));
     CUDA_OK(cudaMalloc(&ddesc_, sizeof(DomainDesc) * (max_domains_ + 1)));
     CUDA_OK(cudaMemset(ddesc_, 0, sizeof(DomainDesc) * (max_domains_ + 1)));
@@ -1131,9 +1473,18 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
     for (int q = 0; q < 2; q++) {
         CUDA_OK(cudaMalloc(&ps.rec[q], capacity_ * sizeof(ActiveRec)));
         CUDA_OK(cudaMalloc(&ps.rdom[q], capacity_ * sizeof(unsigned int)));
+        CUDA_OK(cudaMalloc(&ps.rstat[q], capacity_ * sizeof(unsigned int)));
+        CUDA_OK(cudaMalloc(&ps.rmin2[q], capacity_ * sizeof(unsigned long long)));
     }
-    CUDA_OK(cudaMalloc(&ps.tgt, capacity_ * sizeof(unsigned long long)));
-    CUDA_OK(cudaMalloc(&ps.queue, capacity_ * sizeof(unsigned int)));
+    // a shard takes the entries of 1/kShards of the warps: room for its share of the list plus slack
+    ps.shard_cap = capacity_ / kShards + 8192;
+    const size_t qn = (size_t)kShards * ps.shard_cap;
+    CUDA_OK(cudaMalloc(&ps.tgt, qn * sizeof(unsigned long long)));
+    CUDA_OK(cudaMalloc(&ps.qpos, qn * sizeof(unsigned int)));
+    CUDA_OK(cudaMalloc(&ps.qcell, qn * sizeof(unsigned int)));
+    CUDA_OK(cudaMalloc(&ps.qdom, qn * sizeof(unsigned int)));
+    CUDA_OK(cudaMalloc(&ps.qmask, qn * sizeof(unsigned int)));
+    CUDA_OK(cudaMalloc(&ps.qdl, qn * sizeof(float)));
     ps.capacity = capacity_;
     ps.cur = 0;
     ps.pending = 0;
@@ -1164,9 +1515,15 @@ Pool::~Pool() {
             for (int q = 0; q < 2; q++) {
                 cudaFree(ps.rec[q]);
                 cudaFree(ps.rdom[q]);
+                cudaFree(ps.rstat[q]);
+                cudaFree(ps.rmin2[q]);
             }
             cudaFree(ps.tgt);
-            cudaFree(ps.queue);
+            cudaFree(ps.qpos);
+            cudaFree(ps.qcell);
+            cudaFree(ps.qdom);
+            cudaFree(ps.qmask);
+            cudaFree(ps.qdl);
         }
         cudaFree(dstate_);
     }
@@ -1258,7 +1615,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     d.doc = dalloc<float>(3 * A, s.allocs, s.bytes);
     d.cdl = dalloc<float>(26 * A, s.allocs, s.bytes);
     d.claim = dalloc<unsigned long long>(A, s.allocs, s.bytes);
-    d.lmask = dalloc<unsigned int>(A, s.allocs, s.bytes);
+    d.pos = dalloc<unsigned int>(A, s.allocs, s.bytes);
     // nuclei in time order; ties keep the reference's order (order does not change results)
     size_t P = p.nuclei_loc.size();
     std::vector<int> order(P);
@@ -1279,7 +1636,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     CUDA_OK(cudaMemcpyAsync(d.du, p.du.data(), N * 4, cudaMemcpyHostToDevice, st));
     CUDA_OK(cudaMemsetAsync(d.dl, 0, A * 4, st));
     CUDA_OK(cudaMemsetAsync(d.claim, 0xff, A * 8, st));
-    CUDA_OK(cudaMemsetAsync(d.lmask, 0x80, A * 4, st)); // kMaskFresh in every cell
+    CUDA_OK(cudaMemsetAsync(d.pos, 0xff, A * 4, st)); // kNoRecord
     if (P) {
         CUDA_OK(cudaMemcpyAsync(dnl, nl.data(), P * 4, cudaMemcpyHostToDevice, st));
         CUDA_OK(cudaMemcpyAsync(dnt, nt.data(), P * 4, cudaMemcpyHostToDevice, st));
@@ -1373,50 +1730,33 @@ void Pool::retire(int slot) {
     s = SlotHost();
 }
 
-void Pool::launch_step() {
+// One cooperative launch of k_cycles over n cycles (the grid is exactly the co-resident blocks).
+void Pool::launch_persistent(int n) {
     cudaStream_t st = S(stream_);
-    if (grid_grow_ == 0) {
-        // persistent grids: every resident block slot on the device, grid-stride over the list
-        int b1 = 0, b2 = 0;
-        int b3 = 0, b4 = 0;
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, k_grow, kBlock, 0));
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b2, k_capture, kBlock, 0));
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b3, k_claim, kBlock, 0));
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b4, k_neighbours<true>, kBlock, 0));
-        grid_grow_ = num_sms_ * std::max(b1, 1);
-        grid_capture_ = num_sms_ * std::max(b2, 1);
-        grid_claim_ = num_sms_ * std::max(b3, 1);
-        grid_nb_ = num_sms_ * std::max(b4, 1);
-    }
-    k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
-    k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
-    k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
-    k_capture<<<grid_capture_, kBlock, 0, st>>>(dstate_);
-    k_neighbours<false><<<grid_nb_, kBlock, 0, st>>>(dstate_);
-    launches_ += 5;
+    // the meeting point starts at zero arrivals (a launch that gave up waiting may have left some)
+    CUDA_OK(cudaMemsetAsync((char *)dstate_ + offsetof(PoolState, bar_count), 0, 2 * sizeof(unsigned int), st));
+    PoolState *ps = dstate_;
+    void *args[] = {&ps, &n};
+    CUDA_OK(cudaLaunchCooperativeKernel((const void *)k_cycles, dim3(grid_cycles_), dim3(kBlock), args, 0, st));
+    launches_ += 1;
 }
 
-// n cycles in one stream sequence: the begin of cycles 2..n runs in the tail of the previous
-// capture kernel, so a cycle costs two launches.
-void Pool::launch_cycles(int n) {
-    if (n <= 0)
-        return;
-    if (grid_grow_ == 0)
-        launch_step(), n--; // sizes the grids on first use
+// n cycles as separate pass kernels: the start of cycles 2..n runs in the last block of the
+// previous capture pass, so a cycle costs three launches.
+void Pool::launch_passes(int n) {
     if (n <= 0)
         return;
     cudaStream_t st = S(stream_);
     k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
-    launches_ += 1 + 4ull * n;
     for (int q = 0; q < n; q++) {
         k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
         k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
-        k_capture<<<grid_capture_, kBlock, 0, st>>>(dstate_);
         if (q + 1 < n)
-            k_neighbours<true><<<grid_nb_, kBlock, 0, st>>>(dstate_);
+            k_capture_pass<true><<<grid_capture_, kBlock, 0, st>>>(dstate_);
         else
-            k_neighbours<false><<<grid_nb_, kBlock, 0, st>>>(dstate_);
+            k_capture_pass<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
     }
+    launches_ += 1 + 3ull * n;
 }
 
 void Pool::build_graph() {
@@ -1425,10 +1765,10 @@ void Pool::build_graph() {
     graph_steps_ = 50;
     cudaStream_t st = S(stream_);
     cudaGraph_t graph;
-    if (grid_grow_ == 0)
-        throw DeviceError("grids not sized before graph capture");
     CUDA_OK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-    launch_cycles(graph_steps_);
+    const unsigned long long before = launches_;
+    launch_passes(graph_steps_);
+    launches_ = before;
     CUDA_OK(cudaStreamEndCapture(st, &graph));
     cudaGraphExec_t ex;
     CUDA_OK(cudaGraphInstantiate(&ex, graph, 0));
@@ -1447,17 +1787,18 @@ void Pool::step(int n) {
         slots_[s].steps_launched += n;
         ensure_growth(s, slots_[s].steps_launched + 1);
     }
-    if (grid_grow_ == 0) {
-        launch_step(); // sizes the grids; one cycle
-        n--;
+    if (step_mode_ == 0) {
+        launch_persistent(n);
     }
-    build_graph();
-    cudaStream_t st = S(stream_);
-    int full = n / graph_steps_, rest = n % graph_steps_;
-    for (int q = 0; q < full; q++)
-        CUDA_OK(cudaGraphLaunch((cudaGraphExec_t)graph_exec_, st));
-    launches_ += (unsigned long long)full * (1 + 4ull * graph_steps_);
-    launch_cycles(rest);
+    else {
+        build_graph();
+        cudaStream_t st = S(stream_);
+        const int full = n / graph_steps_, rest = n % graph_steps_;
+        for (int q = 0; q < full; q++)
+            CUDA_OK(cudaGraphLaunch((cudaGraphExec_t)graph_exec_, st));
+        launches_ += (unsigned long long)full * (1 + 3ull * graph_steps_);
+        launch_passes(rest);
+    }
     CUDA_OK(cudaGetLastError());
 }
 
@@ -1513,11 +1854,6 @@ KernelTimes Pool::profile_cycles(int n) {
     KernelTimes kt;
     if (n <= 0)
         return kt;
-    if (grid_grow_ == 0) {
-        launch_step();
-        n--;
-        cycles_launched_++;
-    }
     for (int s = 0; s < (int)slots_.size(); s++) {
         if (!slots_[s].used)
             continue;
@@ -1525,7 +1861,7 @@ KernelTimes Pool::profile_cycles(int n) {
         ensure_growth(s, slots_[s].steps_launched + 1);
     }
     cudaStream_t st = S(stream_);
-    cudaEvent_t ev[6];
+    cudaEvent_t ev[5];
     for (auto &e : ev)
         CUDA_OK(cudaEventCreate(&e));
     for (int q = 0; q < n; q++) {
@@ -1536,26 +1872,78 @@ KernelTimes Pool::profile_cycles(int n) {
         CUDA_OK(cudaEventRecord(ev[2], st));
         k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[3], st));
-        k_capture<<<grid_capture_, kBlock, 0, st>>>(dstate_);
+        k_capture_pass<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[4], st));
-        k_neighbours<false><<<grid_nb_, kBlock, 0, st>>>(dstate_);
-        CUDA_OK(cudaEventRecord(ev[5], st));
-        CUDA_OK(cudaEventSynchronize(ev[5]));
-        float t[5];
-        for (int k = 0; k < 5; k++)
+        CUDA_OK(cudaEventSynchronize(ev[4]));
+        float t[4];
+        for (int k = 0; k < 4; k++)
             CUDA_OK(cudaEventElapsedTime(&t[k], ev[k], ev[k + 1]));
         kt.begin_ms += t[0];
         kt.grow_ms += t[1];
         kt.claim_ms += t[2];
         kt.capture_ms += t[3];
-        kt.neighbours_ms += t[4];
     }
+    CUDA_OK(cudaGetLastError());
     for (auto &e : ev)
         CUDA_OK(cudaEventDestroy(e));
     kt.cycles = n;
-    cycles_launched_ += n;
-    launches_ += 5ull * n;
+    cycles_launched_ += (unsigned long long)n;
+    launches_ += 4ull * n;
     return kt;
+}
+
+void Pool::profile_persistent(int n, double us[7]) {
+    for (int k = 0; k < 7; k++)
+        us[k] = 0;
+    if (n <= 0)
+        return;
+    CUDA_OK(cudaSetDevice(device_));
+    cudaStream_t st = S(stream_);
+    const size_t words = 3 * (3 * (size_t)n + 1);
+    unsigned long long *dtl = nullptr;
+    CUDA_OK(cudaMalloc(&dtl, words * sizeof(unsigned long long)));
+    CUDA_OK(cudaMemsetAsync(dtl, 0, words * sizeof(unsigned long long), st));
+    CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, timeline), &dtl, sizeof(dtl),
+                            cudaMemcpyHostToDevice, st));
+    step(n);
+    unsigned long long *none = nullptr;
+    CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, timeline), &none, sizeof(none),
+                            cudaMemcpyHostToDevice, st));
+    std::vector<unsigned long long> tl(words);
+    CUDA_OK(cudaMemcpyAsync(tl.data(), dtl, words * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaFree(dtl));
+    // meeting points 3c+1, 3c+2, 3c+3 close cycle c's growth, claim and capture passes
+    for (int c = 0; c < n; c++) {
+        const unsigned long long *prev = &tl[3 * (3 * c)], *m1 = &tl[3 * (3 * c + 1)], *m2 = &tl[3 * (3 * c + 2)],
+                                 *m3 = &tl[3 * (3 * c + 3)];
+        us[0] += (double)(m1[0] - prev[2]);
+        us[1] += (double)(m1[1] - prev[2]);
+        us[2] += (double)(m2[0] - m1[2]);
+        us[3] += (double)(m2[1] - m1[2]);
+        us[4] += (double)(m3[0] - m2[2]);
+        us[5] += (double)(m3[1] - m2[2]);
+        us[6] += (double)(m3[2] - m3[1]);
+    }
+    for (int k = 0; k < 7; k++)
+        us[k] /= 1e3 * n;
+}
+
+double Pool::timed_step(int n) {
+    CUDA_OK(cudaSetDevice(device_));
+    cudaStream_t st = S(stream_);
+    cudaEvent_t ev[2];
+    for (auto &e : ev)
+        CUDA_OK(cudaEventCreate(&e));
+    CUDA_OK(cudaEventRecord(ev[0], st));
+    step(n);
+    CUDA_OK(cudaEventRecord(ev[1], st));
+    CUDA_OK(cudaEventSynchronize(ev[1]));
+    float ms = 0;
+    CUDA_OK(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+    for (auto &e : ev)
+        CUDA_OK(cudaEventDestroy(e));
+    return ms;
 }
 
 long long Pool::liquid(int slot) const {

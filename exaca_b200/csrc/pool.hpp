@@ -2,8 +2,8 @@
 //
 // A pool owns a set of independent domains (one for the plain solver, hundreds for batched or
 // served process maps). Every domain's fields live in their own HBM allocations; all domains share
-// one compacted active-cell list, so one launch of each step kernel advances every admitted domain
-// by one CA cycle. The step loop is replayed as a captured CUDA graph.
+// one compacted active-cell list, so one pass of the step kernels advances every admitted domain by
+// one CA cycle; stretches of cycles run in one persistent cooperative launch.
 #pragma once
 
 #include <cstddef>
@@ -19,7 +19,15 @@ namespace exaca {
 
 constexpr int kMaxJumps = 32;
 constexpr unsigned int kTombstone = 0xffffffffu;
+constexpr unsigned int kNoRecord = 0xffffffffu;
 constexpr int kLiquidShards = 16;
+// Per-cycle counters that every warp reserves from are split into kShards counters (warp w uses
+// shard w % kShards), each on its own 64-byte line, so their atomics do not queue on one address.
+constexpr int kShards = 32;
+struct alignas(64) ShardCounter {
+    unsigned long long v;
+    unsigned long long pad[7];
+};
 constexpr int kStatShards = 32;
 // pool statistics, summed over shards
 enum {
@@ -61,7 +69,8 @@ struct DomainDesc {
     float *doc;               // 3 per active-window cell
     float *cdl;               // 26 per active-window cell
     unsigned long long *claim; // per active-window cell: (~epoch << 32) | capturer index
-    unsigned int *lmask;      // per active-window cell: liquid-neighbour directions (kMaskFresh: not known yet)
+    unsigned int *pos;        // per active-window cell: position of its record in the list the next
+                              // cycle reads (kNoRecord for cells that never had one)
     const double *growth;     // growth increment by number of undercooling updates
     const float *guv;         // 9 per orientation
     const float *cdl_table;   // 26 per orientation
@@ -92,11 +101,22 @@ struct DomainDesc {
 struct PoolState {
     ActiveRec *rec[2];           // active-cell records of the current / next cycle
     unsigned int *rdom[2];       // domain of each record
-    unsigned long long *tgt;     // cells claimed this cycle: (domain << 32) | cell
-    unsigned int *queue;         // records the growth pass hands to the claim pass (list positions)
-    unsigned long long qcnt;
+    unsigned int *rstat[2];      // per record: liquid-neighbour directions and flags (kMaskFresh: not built)
+    // per record: (direction of the cached minimum critical length << 32) | second-smallest critical
+    // length (float bits), both over the liquid neighbours not reached at the last claim step
+    unsigned long long *rmin2[2];
+    // claim queue: records the growth pass hands to the claim pass, with the state the claim needs;
+    // shard s holds entries [s * shard_cap, s * shard_cap + qcnt_s[s])
+    unsigned int *qpos, *qcell, *qdom, *qmask;
+    float *qdl;
+    // claims this cycle, (domain << 37) | (direction << 32) | claimed cell; shard s holds entries
+    // [s * shard_cap, s * shard_cap + tcnt_s[s])
+    unsigned long long *tgt;
+    unsigned long long shard_cap;
+    ShardCounter qcnt_s[kShards];
+    ShardCounter tcnt_s[kShards];
+    ShardCounter tomb_s[kShards]; // tombstones added this cycle (summed into tombs at the start of the next)
     unsigned long long cnt[2];
-    unsigned long long tcnt;
     unsigned long long capacity;
     unsigned long long tombs; // dropped records still in list `cur` (in-place cycles)
     int cur;                  // list read by this cycle's growth pass
@@ -107,7 +127,10 @@ struct PoolState {
     int pad;
     DomainDesc *desc;
     unsigned long long stat[kStatShards][kNumStats];
-    unsigned int blocks_done;      // last-block detection of the resolve kernel
+    unsigned int blocks_done;      // last-block detection of the separate capture kernel
+    unsigned int bar_count;        // grid-wide meeting point of the persistent kernel: arrivals
+    unsigned int bar_gen;          // and generation
+    unsigned long long *timeline;  // optional: per meeting point {first arrival, last arrival, release} (ns)
     unsigned long long work[2];    // spare counters
 };
 
@@ -117,9 +140,9 @@ struct PoolStats {
     unsigned long long listed, grown, captured, nucleated, claims, row_reads, dropped, fresh, rechecks, flagged;
 };
 
-// Per-kernel CUDA-event times of a profiled stretch of cycles.
+// CUDA-event times of a stretch of cycles run pass by pass as separate kernels.
 struct KernelTimes {
-    double begin_ms = 0, grow_ms = 0, claim_ms = 0, capture_ms = 0, neighbours_ms = 0;
+    double begin_ms = 0, grow_ms = 0, claim_ms = 0, capture_ms = 0;
     int cycles = 0;
 };
 
@@ -159,7 +182,7 @@ class Pool {
     // the domain on its own; 0 leaves termination to run_plain's host-side census.
     int admit(std::shared_ptr<const Problem> p, int check_mode);
     void retire(int slot);
-    // Advances every unfinished domain by n cycles (graph replay).
+    // Advances every unfinished domain by n cycles (one persistent cooperative launch).
     void step(int n);
     // Reads back the dynamic state of all slots.
     void sync_state();
@@ -175,8 +198,14 @@ class Pool {
     int run_plain(int slot, std::string &log, double *nucl_s, double *capture_s);
     // device time (CUDA events on the pool stream) of the last run_plain
     double last_run_ms() const { return last_run_ms_; }
-    // runs n cycles with a CUDA event around every kernel (no graph), accumulating their times
+    // runs n cycles as separate per-pass kernels with CUDA events around each launch
     KernelTimes profile_cycles(int n);
+    // step(n) with CUDA events around the persistent launch; returns its device time in ms
+    double timed_step(int n);
+    // step(n) with the persistent kernel's timeline on; per-cycle averages in microseconds of
+    // {growth pass: first block done, last block done; claim pass: first, last; capture pass: first,
+    // last; end of cycle and start of the next (last block alone)}
+    void profile_persistent(int n, double us[7]);
     int n_slots() const { return (int)slots_.size(); }
     bool slot_used(int s) const { return s < (int)slots_.size() && slots_[s].used; }
     size_t bytes_in_use() const { return bytes_in_use_; }
@@ -191,8 +220,8 @@ class Pool {
   private:
     void ensure_growth(int slot, long long needed);
     void push_desc(int slot);
-    void launch_step();
-    void launch_cycles(int n);
+    void launch_persistent(int n);
+    void launch_passes(int n); // n cycles as separate pass kernels (stream order)
     void build_graph();
     const DeviceTables &tables_for(const Problem &p);
 
@@ -200,8 +229,6 @@ class Pool {
     size_t budget_;
     size_t bytes_in_use_ = 0;
     void *stream_ = nullptr; // cudaStream_t
-    void *graph_exec_ = nullptr;
-    int graph_steps_ = 0;
     PoolState *dstate_ = nullptr;
     DomainDesc *ddesc_ = nullptr;
     int max_domains_ = 0;
@@ -211,7 +238,11 @@ class Pool {
     std::map<std::string, DeviceTables> tables_;
     int num_sms_ = 148;
     unsigned long long cycles_launched_ = 0;
-    int grid_grow_ = 0, grid_capture_ = 0, grid_claim_ = 0, grid_nb_ = 0;
+    int grid_cycles_ = 0; // co-resident blocks of the persistent kernel
+    int step_mode_ = 0;   // 0: persistent kernel, 1: CUDA graph of the separate pass kernels
+    void *graph_exec_ = nullptr;
+    int graph_steps_ = 0;
+    int grid_grow_ = 0, grid_claim_ = 0, grid_capture_ = 0;
     unsigned long long launches_ = 0;
     double last_run_ms_ = 0;
     void *census_buf_ = nullptr;

@@ -117,8 +117,16 @@ void exaca_pool_destroy(exaca_pool *pool);
  * reference's termination test; 0 leaves it to exaca_pool_run_plain. */
 int exaca_pool_admit(exaca_pool *pool, const exaca_problem *p, int device_check, int *slot);
 /* Advances every unfinished domain by n_cycles CA cycles: Nucleation + CellCapture
- * (src/CAupdate.hpp:15-29) per cycle, replayed as a CUDA graph. Asynchronous. */
+ * (src/CAupdate.hpp:15-29) per cycle, in one persistent kernel launch. Asynchronous. */
 int exaca_pool_step(exaca_pool *pool, int n_cycles);
+/* exaca_pool_step with CUDA events around the launch: waits and returns its device time in ms. */
+int exaca_pool_timed_step(exaca_pool *pool, int n_cycles, double *ms);
+/* exaca_pool_step with the persistent kernel's device timeline on (globaltimer at every grid-wide
+ * meeting point); waits and returns per-cycle averages in microseconds: us[7] = {growth pass done in
+ * the first block, in the last block; claim pass first, last; capture pass first, last; end of the
+ * cycle and start of the next (run by the last block alone)}. Pass times count from the release of
+ * the previous meeting point. */
+int exaca_pool_profile_persistent(exaca_pool *pool, int n_cycles, double *us);
 /* Waits for the device and reads one slot's state. */
 int exaca_pool_status(exaca_pool *pool, int slot, exaca_domain_status *st);
 /* Waits for the device and reads the pool's work counters (summed over all domains). */
@@ -131,9 +139,9 @@ int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c);
 int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cycle);
 /* CUDA-event device time (ms) of the last exaca_pool_run_plain on this pool. */
 double exaca_pool_last_run_ms(exaca_pool *pool);
-/* Runs n_cycles cycles kernel by kernel with CUDA events around each launch (no graph) and returns
- * the summed times in kernel_ms[5] = {cycle start + nucleation, growth pass, claim pass, capture
- * pass, neighbour pass}. */
+/* Runs n_cycles cycles pass by pass as separate kernels with CUDA events around each launch and
+ * returns the summed times in kernel_ms[4] = {cycle start + nucleation, growth pass, claim pass,
+ * capture + neighbour re-check pass}. */
 int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms);
 /* Device->host copy of GrainID and CellType (src/runCA.cpp:423-424); NULL skips a field. */
 int exaca_pool_copy_out(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *cell_type);
