@@ -91,6 +91,7 @@ class CellFieldsT(ctypes.Structure):
 
 
 CENSUS_MAX_DOMAINS = 256
+STEP_CONFIGS = 8
 
 # Every symbol include/exaca_b200.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
@@ -121,6 +122,9 @@ SIGNATURES = {
     "exaca_pool_profile_cycles": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_pool_timed_step": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_pool_profile_persistent": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
+    "exaca_pool_run_all": ([_P, _I, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)], _I),
+    "exaca_pool_set_config": ([_P, _I], _I),
+    "exaca_pool_autotune": ([_P, _I, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_problem_pin": ([_P], _I),
     "exaca_census_cells": ([_I, _P, ctypes.POINTER(CellFieldsT), _I, ctypes.POINTER(CensusT)], _I),
 }
@@ -307,6 +311,23 @@ class Pool:
         _check(load_library().exaca_pool_profile_persistent(self._h, n_cycles, t))
         return {"grow_first": t[0], "grow_last": t[1], "claim_first": t[2], "claim_last": t[3], "capture_first": t[4],
                 "capture_last": t[5], "cycle_end_and_start": t[6]}
+
+    def run_all(self, chunk_cycles: int = 1000, max_cycles: int = 10**7) -> int:
+        """Steps all admitted domains (device_check=True) until each has terminated; returns cycles."""
+        n = ctypes.c_int64()
+        _check(load_library().exaca_pool_run_all(self._h, chunk_cycles, max_cycles, ctypes.byref(n)))
+        return n.value
+
+    def set_config(self, config: int) -> None:
+        _check(load_library().exaca_pool_set_config(self._h, config))
+
+    def autotune(self, trial_cycles: int = 100):
+        """Times every step configuration on trial_cycles real cycles; keeps and returns the fastest
+        (config, ms per cycle of every configuration)."""
+        c = ctypes.c_int()
+        t = (ctypes.c_double * STEP_CONFIGS)()
+        _check(load_library().exaca_pool_autotune(self._h, trial_cycles, ctypes.byref(c), t))
+        return c.value, list(t)
 
     def timed_step(self, n_cycles: int) -> float:
         """step(n_cycles) (one persistent launch) timed with CUDA events; waits; returns ms."""

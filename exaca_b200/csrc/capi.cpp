@@ -271,6 +271,32 @@ int exaca_pool_profile_persistent(exaca_pool *pool, int n_cycles, double *us) {
     return guarded([&] { pool->pool->profile_persistent(n_cycles, us); });
 }
 
+int exaca_pool_run_all(exaca_pool *pool, int chunk_cycles, int64_t max_cycles, int64_t *cycles_stepped) {
+    if (!pool || chunk_cycles <= 0 || max_cycles < 0)
+        return fail(EXACA_ERR_ARG, "bad argument");
+    return guarded([&] {
+        long long n = pool->pool->run_all(chunk_cycles, max_cycles);
+        if (cycles_stepped)
+            *cycles_stepped = n;
+    });
+}
+
+int exaca_pool_set_config(exaca_pool *pool, int config) {
+    if (!pool || config < 0 || config >= exaca::Pool::kStepConfigs)
+        return fail(EXACA_ERR_ARG, "step configuration out of range");
+    return guarded([&] { pool->pool->set_config(config); });
+}
+
+int exaca_pool_autotune(exaca_pool *pool, int trial_cycles, int *config, double *ms_per_cycle) {
+    if (!pool || trial_cycles <= 0)
+        return fail(EXACA_ERR_ARG, "bad argument");
+    return guarded([&] {
+        int c = pool->pool->autotune(trial_cycles, ms_per_cycle);
+        if (config)
+            *config = c;
+    });
+}
+
 int exaca_pool_timed_step(exaca_pool *pool, int n_cycles, double *ms) {
     if (!pool || !ms || n_cycles < 0)
         return fail(EXACA_ERR_ARG, "bad argument");

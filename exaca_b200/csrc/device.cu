@@ -518,8 +518,11 @@ __global__ void k_step_begin(PoolState *P) { begin_cycle(P); }
 // They run as three kernels per cycle (k_grow, k_claim, k_capture_pass) or, for stretches of
 // cycles, inside the persistent cooperative kernel k_cycles with grid-wide barriers between them.
 constexpr unsigned int kNeedsClaim = 0xffffffffu; // NaN pattern in ActiveRec::cdl_min
-constexpr int kBatch = 4;
-constexpr int kCaptureLanes = 8;
+// Launch-shape parameters (template arguments of the passes; the pool's tuner picks among the
+// compiled combinations): records per lane in flight in the growth pass, lanes per claim in the
+// capture pass.
+constexpr int kBatchChoices[2] = {2, 4};
+constexpr int kLaneChoices[2] = {4, 8};
 constexpr int kErrBarrier = 8;
 
 struct CycleStats {
@@ -696,6 +699,7 @@ __device__ __forceinline__ unsigned int claim_entry(PoolState *P, ActiveRec *rec
 }
 
 // Puts the flagged records of one growth step into the claim queue (all lanes of the warp call).
+template <int kBatch>
 __device__ __forceinline__ void queue_flagged(PoolState *P, unsigned int shard, unsigned int nf, unsigned int flagged,
                                               const unsigned long long *idx, const ActiveRec *r,
                                               const unsigned int *dom, const unsigned int *m) {
@@ -765,7 +769,7 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
         }
         const bool flag = placed && __float_as_uint(r.cdl_min) == kNeedsClaim;
         unsigned long long idx = pos;
-        queue_flagged(P, (unsigned int)(gw % kShards), flag ? 1u : 0u, flag ? 1u : 0u, &idx, &r, &dom, &m);
+        queue_flagged<1>(P, (unsigned int)(gw % kShards), flag ? 1u : 0u, flag ? 1u : 0u, &idx, &r, &dom, &m);
     }
 }
 
@@ -773,7 +777,7 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
 // group g to warp g % (number of warps of the grid), consecutive warps on different blocks: the
 // records appended by the last capture pass, which all need a fresh mask and claims, spread over
 // every SM. No block-wide synchronisation.
-__device__ void grow_pass(PoolState *P, CycleStats &st) {
+template <int kBatch> __device__ void grow_pass(PoolState *P, CycleStats &st) {
     const int cur = P->cur;
     const unsigned long long n = P->cnt[cur];
     const unsigned int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -844,7 +848,7 @@ __device__ void grow_pass(PoolState *P, CycleStats &st) {
                     flagged |= 1u << q;
             }
         }
-        queue_flagged(P, (unsigned int)(gw % kShards), __popc(flagged), flagged, idx, r, dom, m);
+        queue_flagged<kBatch>(P, (unsigned int)(gw % kShards), __popc(flagged), flagged, idx, r, dom, m);
     }
     // dropped records stay as tombstones of the in-place list until the next compaction
 #pragma unroll
@@ -927,7 +931,7 @@ __device__ void claim_pass(PoolState *P, CycleStats &st) {
     }
 }
 
-__device__ void capture_pass(PoolState *P, CycleStats &st) {
+template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleStats &st) {
     __shared__ unsigned long long s_pre[kShards + 1];
     shard_prefix(P->tcnt_s, s_pre);
     const int app = P->pending; // list of the next cycle
@@ -1071,9 +1075,9 @@ __device__ void finish_capture(PoolState *P) {
     __syncthreads();
 }
 
-__global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
+template <int kBatch> __global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
     CycleStats st;
-    grow_pass(P, st);
+    grow_pass<kBatch>(P, st);
     flush_stats(P, st);
 }
 
@@ -1085,9 +1089,9 @@ __global__ void __launch_bounds__(kBlock) k_claim(PoolState *P) {
 
 // Capture pass as its own kernel; the last block to finish closes the cycle and, with kBegin,
 // starts the next one.
-template <bool kBegin> __global__ void __launch_bounds__(kBlock) k_capture_pass(PoolState *P) {
+template <bool kBegin, int kLanes> __global__ void __launch_bounds__(kBlock) k_capture_pass(PoolState *P) {
     CycleStats st;
-    capture_pass(P, st);
+    capture_pass<kLanes>(P, st);
     flush_stats(P, st);
     __shared__ int s_last;
     __threadfence(); // this block's writes are visible device-wide before it is counted
@@ -1184,11 +1188,11 @@ template <class F> __device__ bool grid_meet(PoolState *P, int tag, F &&serial) 
 }
 
 // n_cycles complete CA cycles (start, grow/claim, capture) in one cooperative launch.
-__global__ void __launch_bounds__(kBlock, 2) k_cycles(PoolState *P, int n_cycles) {
+template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 2) k_cycles(PoolState *P, int n_cycles) {
     CycleStats st;
     bool ok = grid_meet(P, 0, [&] { begin_cycle(P); });
     for (int c = 0; ok && c < n_cycles; c++) {
-        grow_pass(P, st);
+        grow_pass<kBatch>(P, st);
         ok = grid_meet(P, 3 * c + 1, [] {});
         if (!ok)
             break;
@@ -1196,7 +1200,7 @@ __global__ void __launch_bounds__(kBlock, 2) k_cycles(PoolState *P, int n_cycles
         ok = grid_meet(P, 3 * c + 2, [] {});
         if (!ok)
             break;
-        capture_pass(P, st);
+        capture_pass<kLanes>(P, st);
         const bool more = c + 1 < n_cycles;
         ok = grid_meet(P, 3 * c + 3, [&] {
             finish_capture(P);
@@ -1206,6 +1210,21 @@ __global__ void __launch_bounds__(kBlock, 2) k_cycles(PoolState *P, int n_cycles
     }
     flush_stats(P, st);
 }
+
+// Compiled launch shapes: {capture lanes, growth batch} for kLaneChoices x kBatchChoices.
+struct StepKernels {
+    const void *cycles;
+    void (*grow)(PoolState *);
+    void (*capture_begin)(PoolState *);
+    void (*capture_end)(PoolState *);
+};
+template <int kL, int kB> StepKernels step_kernels() {
+    return {(const void *)k_cycles<kL, kB>, k_grow<kB>, k_capture_pass<true, kL>, k_capture_pass<false, kL>};
+}
+static_assert(kStepVariants == 4, "two lane widths x two batch depths");
+const StepKernels kStepKernel[kStepVariants] = {
+    step_kernels<kLaneChoices[0], kBatchChoices[0]>(), step_kernels<kLaneChoices[0], kBatchChoices[1]>(),
+    step_kernels<kLaneChoices[1], kBatchChoices[0]>(), step_kernels<kLaneChoices[1], kBatchChoices[1]>()};
 
 // ---------------------------------------------------------------------------------------------
 // Census of src/CAupdate.cpp:738-808 for one domain (layer 0 is the only layer).
@@ -1446,16 +1465,18 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
     if (!coop)
         throw DeviceError("device does not support cooperative launches");
     int b = 0;
-    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_cycles, kBlock, 0));
-    if (b < 1)
-        throw DeviceError("persistent kernel does not fit on an SM");
-    grid_cycles_ = num_sms_ * b;
-    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_grow, kBlock, 0));
-    grid_grow_ = num_sms_ * std::max(b, 1);
+    for (int v = 0; v < kStepVariants; v++) {
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kStepKernel[v].cycles, kBlock, 0));
+        if (b < 1)
+            throw DeviceError("persistent kernel does not fit on an SM");
+        grid_cycles_[v] = num_sms_ * b;
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void *)kStepKernel[v].grow, kBlock, 0));
+        grid_grow_[v] = num_sms_ * std::max(b, 1);
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, (const void *)kStepKernel[v].capture_end, kBlock, 0));
+        grid_capture_[v] = num_sms_ * std::max(b, 1);
+    }
     CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_claim, kBlock, 0));
     grid_claim_ = num_sms_ * std::max(b, 1);
-    CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_capture_pass<false>, kBlock, 0));
-    grid_capture_ = num_sms_ * std::max(b, 1);
     if (const char *m = std::getenv("EXACA_STEP_MODE"))
         step_mode_ = std::string(m) == "graph" ? 1 : 0;
     CUDA_OK(cudaMalloc(&dstate_, sizeof(PoolState)));
@@ -1737,7 +1758,8 @@ void Pool::launch_persistent(int n) {
     CUDA_OK(cudaMemsetAsync((char *)dstate_ + offsetof(PoolState, bar_count), 0, 2 * sizeof(unsigned int), st));
     PoolState *ps = dstate_;
     void *args[] = {&ps, &n};
-    CUDA_OK(cudaLaunchCooperativeKernel((const void *)k_cycles, dim3(grid_cycles_), dim3(kBlock), args, 0, st));
+    CUDA_OK(cudaLaunchCooperativeKernel(kStepKernel[variant_].cycles, dim3(grid_cycles_[variant_]), dim3(kBlock), args,
+                                        0, st));
     launches_ += 1;
 }
 
@@ -1747,14 +1769,15 @@ void Pool::launch_passes(int n) {
     if (n <= 0)
         return;
     cudaStream_t st = S(stream_);
+    const StepKernels &K = kStepKernel[variant_];
     k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
     for (int q = 0; q < n; q++) {
-        k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+        K.grow<<<grid_grow_[variant_], kBlock, 0, st>>>(dstate_);
         k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
         if (q + 1 < n)
-            k_capture_pass<true><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+            K.capture_begin<<<grid_capture_[variant_], kBlock, 0, st>>>(dstate_);
         else
-            k_capture_pass<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+            K.capture_end<<<grid_capture_[variant_], kBlock, 0, st>>>(dstate_);
     }
     launches_ += 1 + 3ull * n;
 }
@@ -1868,11 +1891,11 @@ KernelTimes Pool::profile_cycles(int n) {
         CUDA_OK(cudaEventRecord(ev[0], st));
         k_step_begin<<<1, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[1], st));
-        k_grow<<<grid_grow_, kBlock, 0, st>>>(dstate_);
+        kStepKernel[variant_].grow<<<grid_grow_[variant_], kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[2], st));
         k_claim<<<grid_claim_, kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[3], st));
-        k_capture_pass<false><<<grid_capture_, kBlock, 0, st>>>(dstate_);
+        kStepKernel[variant_].capture_end<<<grid_capture_[variant_], kBlock, 0, st>>>(dstate_);
         CUDA_OK(cudaEventRecord(ev[4], st));
         CUDA_OK(cudaEventSynchronize(ev[4]));
         float t[4];
@@ -1927,6 +1950,67 @@ void Pool::profile_persistent(int n, double us[7]) {
     }
     for (int k = 0; k < 7; k++)
         us[k] /= 1e3 * n;
+}
+
+void Pool::set_config(int config) {
+    if (config < 0 || config >= kStepConfigs)
+        throw std::invalid_argument("step configuration out of range");
+    const int mode = config / kStepVariants, variant = config % kStepVariants;
+    if (variant != variant_ && graph_exec_) {
+        CUDA_OK(cudaStreamSynchronize(S(stream_)));
+        CUDA_OK(cudaGraphExecDestroy((cudaGraphExec_t)graph_exec_));
+        graph_exec_ = nullptr;
+    }
+    step_mode_ = mode;
+    variant_ = variant;
+}
+
+int Pool::autotune(int trial_cycles, double *ms_per_cycle) {
+    int best = config();
+    double best_ms = 1e300;
+    for (int c = 0; c < kStepConfigs; c++) {
+        set_config(c);
+        if (step_mode_ == 1)
+            build_graph(); // outside the timed trial
+        const double ms = timed_step(trial_cycles) / std::max(trial_cycles, 1);
+        if (ms_per_cycle)
+            ms_per_cycle[c] = ms;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    set_config(best);
+    return best;
+}
+
+long long Pool::run_all(int chunk, long long max_cycles) {
+    if (chunk <= 0)
+        throw std::invalid_argument("chunk must be positive");
+    long long stepped = 0;
+    while (true) {
+        sync_state();
+        bool all_done = true;
+        for (int s = 0; s < (int)slots_.size(); s++) {
+            if (!slots_[s].used)
+                continue;
+            const DomainDesc &d = host_desc_[s];
+            if (d.error)
+                throw DeviceError("device error flags " + std::to_string(d.error) + " in slot " + std::to_string(s));
+            if (!d.check_mode)
+                throw std::invalid_argument("slot " + std::to_string(s) + " was admitted without device termination");
+            all_done = all_done && d.done;
+        }
+        const int perr = pool_error();
+        if (perr)
+            throw DeviceError("pool error flags " + std::to_string(perr));
+        if (all_done)
+            return stepped;
+        if (stepped >= max_cycles)
+            throw DeviceError("domains still running after " + std::to_string(stepped) + " cycles");
+        step(chunk);
+        stepped += chunk;
+    }
 }
 
 double Pool::timed_step(int n) {

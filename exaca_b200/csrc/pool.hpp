@@ -18,6 +18,7 @@
 namespace exaca {
 
 constexpr int kMaxJumps = 32;
+constexpr int kStepVariants = 4; // compiled launch shapes of the step passes
 constexpr unsigned int kTombstone = 0xffffffffu;
 constexpr unsigned int kNoRecord = 0xffffffffu;
 constexpr int kLiquidShards = 16;
@@ -200,8 +201,18 @@ class Pool {
     double last_run_ms() const { return last_run_ms_; }
     // runs n cycles as separate per-pass kernels with CUDA events around each launch
     KernelTimes profile_cycles(int n);
-    // step(n) with CUDA events around the persistent launch; returns its device time in ms
+    // step(n) with CUDA events around the launches; returns their device time in ms
     double timed_step(int n);
+    // Step configurations: config = mode * kStepVariants + variant. set_config switches; autotune
+    // runs trial_cycles real cycles with every configuration (the pool's domains advance), keeps
+    // the fastest and returns it; ms_per_cycle (kStepConfigs entries, may be null) gets the trials.
+    static constexpr int kStepConfigs = 2 * kStepVariants;
+    void set_config(int config);
+    int config() const { return step_mode_ * kStepVariants + variant_; }
+    int autotune(int trial_cycles, double *ms_per_cycle);
+    // Steps every admitted domain in chunks of `chunk` cycles until each one has ended on the device
+    // (admitted with check_mode 1); returns the cycles stepped. Throws past max_cycles.
+    long long run_all(int chunk, long long max_cycles);
     // step(n) with the persistent kernel's timeline on; per-cycle averages in microseconds of
     // {growth pass: first block done, last block done; claim pass: first, last; capture pass: first,
     // last; end of cycle and start of the next (last block alone)}
@@ -238,11 +249,16 @@ class Pool {
     std::map<std::string, DeviceTables> tables_;
     int num_sms_ = 148;
     unsigned long long cycles_launched_ = 0;
-    int grid_cycles_ = 0; // co-resident blocks of the persistent kernel
-    int step_mode_ = 0;   // 0: persistent kernel, 1: CUDA graph of the separate pass kernels
+    // step configuration: mode (0: persistent kernel, 1: CUDA graph of the separate pass kernels)
+    // x launch-shape variant (kStepVariants compiled lane / batch combinations)
+    int step_mode_ = 0;
+    int variant_ = kStepVariants - 1;
+    int grid_cycles_[kStepVariants] = {}; // co-resident blocks of each persistent kernel
+    int grid_grow_[kStepVariants] = {};
+    int grid_capture_[kStepVariants] = {};
     void *graph_exec_ = nullptr;
     int graph_steps_ = 0;
-    int grid_grow_ = 0, grid_claim_ = 0, grid_capture_ = 0;
+    int grid_claim_ = 0;
     unsigned long long launches_ = 0;
     double last_run_ms_ = 0;
     void *census_buf_ = nullptr;

@@ -119,6 +119,19 @@ int exaca_pool_admit(exaca_pool *pool, const exaca_problem *p, int device_check,
 /* Advances every unfinished domain by n_cycles CA cycles: Nucleation + CellCapture
  * (src/CAupdate.hpp:15-29) per cycle, in one persistent kernel launch. Asynchronous. */
 int exaca_pool_step(exaca_pool *pool, int n_cycles);
+/* Batched solve (no counterpart in the reference): steps every admitted domain in chunks of
+ * chunk_cycles until each has met the reference's termination test on the device (all slots must
+ * be admitted with device_check = 1; type-C problems, whose run has no cycle jump). A domain's
+ * result does not depend on the other domains in the pool. */
+int exaca_pool_run_all(exaca_pool *pool, int chunk_cycles, int64_t max_cycles, int64_t *cycles_stepped);
+/* Step configurations (no counterpart in the reference): config = mode * 4 + shape, mode 0 the
+ * persistent kernel and 1 a CUDA graph of the per-pass kernels, shape one of the compiled
+ * {capture lanes 4|8} x {growth records per lane 2|4}. Results do not depend on the configuration. */
+#define EXACA_STEP_CONFIGS 8
+int exaca_pool_set_config(exaca_pool *pool, int config);
+/* Autotuner: runs trial_cycles real cycles of the pool's domains in every configuration, keeps the
+ * fastest; ms_per_cycle (EXACA_STEP_CONFIGS entries, may be NULL) receives the trial times. */
+int exaca_pool_autotune(exaca_pool *pool, int trial_cycles, int *config, double *ms_per_cycle);
 /* exaca_pool_step with CUDA events around the launch: waits and returns its device time in ms. */
 int exaca_pool_timed_step(exaca_pool *pool, int n_cycles, double *ms);
 /* exaca_pool_step with the persistent kernel's device timeline on (globaltimer at every grid-wide
