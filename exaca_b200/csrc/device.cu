@@ -1313,6 +1313,8 @@ __global__ void k_voronoi(DomainDesc *Dp, const int32_t *seeds, int nseeds, floa
 
 // Initially active cells: fresh octahedra and the first records (src/CAinitialize.cpp:1929-2044).
 __global__ void k_init_active(PoolState *P, int dom, int list_slot) {
+    if (list_slot < 0)
+        list_slot = P->pending; // the list the next cycle consumes
     DomainDesc &D = P->desc[dom];
     long long plane = (long long)D.mx * D.my;
     long long lo = plane, hi = plane * (D.nz - 1);
@@ -1566,8 +1568,8 @@ const DeviceTables &Pool::tables_for(const Problem &p) {
 }
 
 void Pool::push_desc(int slot) {
+    // pageable source: staged before the call returns
     CUDA_OK(cudaMemcpyAsync(ddesc_ + slot, &host_desc_[slot], sizeof(DomainDesc), cudaMemcpyHostToDevice, S(stream_)));
-    CUDA_OK(cudaStreamSynchronize(S(stream_)));
 }
 
 void Pool::ensure_growth(int slot, long long needed) {
@@ -1581,10 +1583,12 @@ void Pool::ensure_growth(int slot, long long needed) {
     build_growth_table(*s.problem, (int)len, g);
     double *d = nullptr;
     CUDA_OK(cudaMalloc(&d, len * sizeof(double)));
-    CUDA_OK(cudaMemcpy(d, g.data(), len * sizeof(double), cudaMemcpyHostToDevice));
-    CUDA_OK(cudaStreamSynchronize(S(stream_)));
-    if (s.growth)
+    CUDA_OK(cudaMemcpyAsync(d, g.data(), len * sizeof(double), cudaMemcpyHostToDevice, S(stream_)));
+    if (s.growth) {
+        // the old table may still be read by queued work
+        CUDA_OK(cudaStreamSynchronize(S(stream_)));
         CUDA_OK(cudaFree(s.growth));
+    }
     s.growth = d;
     s.growth_len = (int)len;
     // patch only the table fields of the device descriptor
@@ -1595,7 +1599,6 @@ void Pool::ensure_growth(int slot, long long needed) {
                             cudaMemcpyHostToDevice, S(stream_)));
     CUDA_OK(cudaMemcpyAsync((char *)(ddesc_ + slot) + offsetof(DomainDesc, growth_len), &h.growth_len,
                             sizeof(h.growth_len), cudaMemcpyHostToDevice, S(stream_)));
-    CUDA_OK(cudaStreamSynchronize(S(stream_)));
 }
 
 int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
@@ -1624,21 +1627,36 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     s.used = true;
     s.problem = pp;
     const Geometry &g = p.g;
-    size_t N = g.domain_size, A = g.active_size;
+    const size_t N = g.domain_size, A = g.active_size, P = p.nuclei_loc.size();
+    // every field of the slot in one allocation (256-byte aligned sub-arrays)
+    size_t off = 0;
+    auto carve = [&](size_t bytes) {
+        size_t o = off;
+        off += (std::max<size_t>(bytes, 16) + 255) & ~(size_t)255;
+        return o;
+    };
+    const size_t o_ct = carve(N), o_gid = carve(N * 4), o_cts = carve(N * 4), o_ly = carve(N), o_du = carve(N * 4),
+                 o_dl = carve(A * 4), o_doc = carve(A * 12), o_cdl = carve(A * 104), o_claim = carve(A * 8),
+                 o_pos = carve(A * 4), o_nl = carve(P * 4), o_nt = carve(P * 4);
+    char *slab = nullptr;
+    CUDA_OK(cudaMalloc(&slab, off));
+    s.allocs.push_back(slab);
+    s.bytes = off;
     DomainDesc d;
     std::memset(&d, 0, sizeof(d));
-    d.ctype = dalloc<int8_t>(N, s.allocs, s.bytes);
-    d.gid = dalloc<int32_t>(N, s.allocs, s.bytes);
-    d.cts = dalloc<int32_t>(N, s.allocs, s.bytes);
-    d.layer = dalloc<int8_t>(N, s.allocs, s.bytes);
-    d.du = dalloc<float>(N, s.allocs, s.bytes);
-    d.dl = dalloc<float>(A, s.allocs, s.bytes);
-    d.doc = dalloc<float>(3 * A, s.allocs, s.bytes);
-    d.cdl = dalloc<float>(26 * A, s.allocs, s.bytes);
-    d.claim = dalloc<unsigned long long>(A, s.allocs, s.bytes);
-    d.pos = dalloc<unsigned int>(A, s.allocs, s.bytes);
+    d.ctype = (int8_t *)(slab + o_ct);
+    d.gid = (int32_t *)(slab + o_gid);
+    d.cts = (int32_t *)(slab + o_cts);
+    d.layer = (int8_t *)(slab + o_ly);
+    d.du = (float *)(slab + o_du);
+    d.dl = (float *)(slab + o_dl);
+    d.doc = (float *)(slab + o_doc);
+    d.cdl = (float *)(slab + o_cdl);
+    d.claim = (unsigned long long *)(slab + o_claim);
+    d.pos = (unsigned int *)(slab + o_pos);
+    int32_t *dnl = (int32_t *)(slab + o_nl);
+    int32_t *dnt = (int32_t *)(slab + o_nt);
     // nuclei in time order; ties keep the reference's order (order does not change results)
-    size_t P = p.nuclei_loc.size();
     std::vector<int> order(P);
     std::iota(order.begin(), order.end(), 0);
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return p.nuclei_time[a] < p.nuclei_time[b]; });
@@ -1647,8 +1665,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
         nl[q] = p.nuclei_loc[order[q]];
         nt[q] = p.nuclei_time[order[q]];
     }
-    int32_t *dnl = dalloc<int32_t>(P, s.allocs, s.bytes);
-    int32_t *dnt = dalloc<int32_t>(P, s.allocs, s.bytes);
+    // host->device copies on the pool stream; pageable sources are staged before each call returns
     cudaStream_t st = S(stream_);
     CUDA_OK(cudaMemcpyAsync(d.ctype, p.cell_type.data(), N, cudaMemcpyHostToDevice, st));
     CUDA_OK(cudaMemcpyAsync(d.gid, p.grain_id.data(), N * 4, cudaMemcpyHostToDevice, st));
@@ -1705,21 +1722,17 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
         k_voronoi<<<(unsigned)blocks, 256, 3 * 1024 * sizeof(int), st>>>(ddesc_ + slot, dseeds, nseeds,
                                                                          (float)(g.active_size));
         CUDA_OK(cudaGetLastError());
-        CUDA_OK(cudaStreamSynchronize(st));
-        if (dseeds)
+        if (dseeds) {
+            CUDA_OK(cudaStreamSynchronize(st));
             CUDA_OK(cudaFree(dseeds));
+        }
     }
     // register the domain, then build its initial active list in the list the next cycle consumes
-    PoolState ps;
-    CUDA_OK(cudaMemcpyAsync(&ps, dstate_, sizeof(ps), cudaMemcpyDeviceToHost, st));
-    CUDA_OK(cudaStreamSynchronize(st));
-    int n_domains = std::max(ps.n_domains, slot + 1);
-    CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, n_domains), &n_domains, sizeof(int),
+    n_domains_ = std::max(n_domains_, slot + 1);
+    CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, n_domains), &n_domains_, sizeof(int),
                             cudaMemcpyHostToDevice, st));
-    int next_slot = ps.pending;
-    k_init_active<<<num_sms_ * 4, 256, 0, st>>>(dstate_, slot, next_slot);
+    k_init_active<<<num_sms_ * 4, 256, 0, st>>>(dstate_, slot, -1);
     CUDA_OK(cudaGetLastError());
-    CUDA_OK(cudaStreamSynchronize(st));
     bytes_in_use_ += s.bytes;
     return slot;
 }
@@ -1805,7 +1818,8 @@ void Pool::step(int n) {
     cycles_launched_ += (unsigned long long)n;
     CUDA_OK(cudaSetDevice(device_));
     for (int s = 0; s < (int)slots_.size(); s++) {
-        if (!slots_[s].used)
+        // a domain known to have ended executes no further cycle
+        if (!slots_[s].used || host_desc_[s].done)
             continue;
         slots_[s].steps_launched += n;
         ensure_growth(s, slots_[s].steps_launched + 1);

@@ -243,6 +243,7 @@ class Pool {
     PoolState *dstate_ = nullptr;
     DomainDesc *ddesc_ = nullptr;
     int max_domains_ = 0;
+    int n_domains_ = 0; // highest used slot + 1 (mirrors PoolState::n_domains)
     unsigned long long capacity_ = 0;
     std::vector<SlotHost> slots_;
     std::vector<DomainDesc> host_desc_;
