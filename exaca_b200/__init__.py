@@ -123,6 +123,7 @@ SIGNATURES = {
     "exaca_pool_timed_step": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_pool_profile_persistent": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_pool_run_all": ([_P, _I, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)], _I),
+    "exaca_pool_status_many": ([_P, _I, ctypes.POINTER(_I), ctypes.POINTER(DomainStatus)], _I),
     "exaca_pool_set_config": ([_P, _I], _I),
     "exaca_pool_autotune": ([_P, _I, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_problem_pin": ([_P], _I),
@@ -264,6 +265,14 @@ class Pool:
         s = DomainStatus()
         _check(load_library().exaca_pool_status(self._h, slot, ctypes.byref(s)))
         return Status(s.cycle, bool(s.done), s.nn, s.error, s.liquid)
+
+    def status_many(self, slots) -> list:
+        """status() of several slots with one device read."""
+        n = len(slots)
+        arr = (_I * max(n, 1))(*slots)
+        out = (DomainStatus * max(n, 1))()
+        _check(load_library().exaca_pool_status_many(self._h, n, arr, out))
+        return [Status(s.cycle, bool(s.done), s.nn, s.error, s.liquid) for s in out[:n]]
 
     def stats(self) -> dict:
         s = PoolStatsT()

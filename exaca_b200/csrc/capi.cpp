@@ -231,6 +231,26 @@ int exaca_pool_status(exaca_pool *pool, int slot, exaca_domain_status *st) {
     });
 }
 
+int exaca_pool_status_many(exaca_pool *pool, int n_slots, const int *slots, exaca_domain_status *st) {
+    if (!pool || n_slots < 0 || (n_slots && (!slots || !st)))
+        return fail(EXACA_ERR_ARG, "null argument");
+    for (int i = 0; i < n_slots; i++)
+        if (!pool->pool->slot_used(slots[i]))
+            return fail(EXACA_ERR_ARG, "bad slot " + std::to_string(slots[i]));
+    return guarded([&] {
+        pool->pool->sync_state();
+        const int perr = pool->pool->pool_error();
+        for (int i = 0; i < n_slots; i++) {
+            const exaca::DomainDesc &d = pool->pool->state(slots[i]);
+            st[i].cycle = d.cycle;
+            st[i].done = d.done;
+            st[i].nn = d.nn;
+            st[i].error = d.error | perr;
+            st[i].liquid = pool->pool->liquid(slots[i]);
+        }
+    });
+}
+
 int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st) {
     if (!pool || !st)
         return fail(EXACA_ERR_ARG, "null argument");

@@ -142,6 +142,8 @@ int exaca_pool_timed_step(exaca_pool *pool, int n_cycles, double *ms);
 int exaca_pool_profile_persistent(exaca_pool *pool, int n_cycles, double *us);
 /* Waits for the device and reads one slot's state. */
 int exaca_pool_status(exaca_pool *pool, int slot, exaca_domain_status *st);
+/* exaca_pool_status for n_slots slots with one device read (request loops poll many domains). */
+int exaca_pool_status_many(exaca_pool *pool, int n_slots, const int *slots, exaca_domain_status *st);
 /* Waits for the device and reads the pool's work counters (summed over all domains). */
 int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st);
 /* IntermediateOutputAndCheck's census (src/CAupdate.hpp:30-33) for one slot. */
