@@ -388,8 +388,8 @@ __device__ void drop_from_neighbour_masks(const DomainDesc &D, unsigned int *rst
 // Start of a CA cycle for every domain (src/runCA.cpp:290-298, src/CAupdate.cpp:67-200), run by one
 // block: list swap, device-side termination check, cycle advance, nucleation. Reads that may see
 // data other blocks of the same kernel wrote go through L2 (__ldcg).
-__device__ __noinline__ void begin_cycle(PoolState *P) {
-    __shared__ int s_cur;
+// Start of a cycle, pool part (one warp): list swap, compaction decision, per-cycle counters.
+__device__ __noinline__ void begin_lists(PoolState *P) {
     if (threadIdx.x < 32) {
         // the list the previous cycle left becomes current; when it was a compacted copy, the old
         // one is emptied and carries no dropped records any more (all loads issued together)
@@ -420,14 +420,17 @@ __device__ __noinline__ void begin_cycle(PoolState *P) {
             P->pending = compact ? cur ^ 1 : cur;
             if (compact)
                 P->cnt[cur ^ 1] = 0;
-            s_cur = cur;
         }
     }
-    __syncthreads();
-    const int cur = s_cur;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+}
+
+// Start of a cycle, per-domain part: warps first_warp, first_warp + warp_stride, ... take one
+// domain each (the current list must already be settled by begin_lists).
+__device__ __noinline__ void begin_domains(PoolState *P, int first_warp, int warp_stride) {
+    const int cur = P->cur;
+    const int lane = threadIdx.x & 31;
     unsigned long long nucleated = 0;
-    for (int d = warp; d < P->n_domains; d += nwarps) {
+    for (int d = first_warp; d < P->n_domains; d += warp_stride) {
         DomainDesc &D = P->desc[d];
         if (D.ctype == nullptr || D.done)
             continue;
@@ -499,6 +502,13 @@ __device__ __noinline__ void begin_cycle(PoolState *P) {
     }
     if (lane == 0 && nucleated)
         atomicAdd(&P->stat[0][kStatNucleated], nucleated);
+}
+
+// Start of a cycle by one block (the pool part, then every domain with the block's warps).
+__device__ __noinline__ void begin_cycle(PoolState *P) {
+    begin_lists(P);
+    __syncthreads();
+    begin_domains(P, threadIdx.x >> 5, blockDim.x >> 5);
 }
 
 __global__ void k_step_begin(PoolState *P) { begin_cycle(P); }
@@ -1118,6 +1128,7 @@ template <bool kBegin, int kLanes> __global__ void __launch_bounds__(kBlock) k_c
 // wait is bounded: after kMeetTimeoutNs (or kMeetSpinCap polls) the block sets kErrBarrier and
 // the kernel ends.
 constexpr unsigned long long kMeetTimeoutNs = 1000000000ull;
+constexpr int kSerialDomains = 8; // up to this many domains one block starts each cycle alone
 constexpr unsigned int kMeetSpinCap = 1u << 26;
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
@@ -1147,7 +1158,7 @@ template <class F> __device__ bool grid_meet(PoolState *P, int tag, F &&serial) 
     if (threadIdx.x == 0) {
         const unsigned int gen = ld_acquire_u32(&P->bar_gen);
         const unsigned int prev = atom_add_acq_rel_u32(&P->bar_count, 1u);
-        unsigned long long *tl = P->timeline;
+        unsigned long long *tl = tag >= 0 ? P->timeline : nullptr;
         if (tl && prev == 0)
             tl[3 * tag + 0] = global_ns();
         int state = 0;
@@ -1178,7 +1189,7 @@ template <class F> __device__ bool grid_meet(PoolState *P, int tag, F &&serial) 
         serial();
         __syncthreads();
         if (threadIdx.x == 0) {
-            if (P->timeline)
+            if (P->timeline && tag >= 0)
                 P->timeline[3 * tag + 2] = global_ns();
             P->bar_count = 0;
             st_release_u32(&P->bar_gen, s_gen + 1u);
@@ -1190,7 +1201,19 @@ template <class F> __device__ bool grid_meet(PoolState *P, int tag, F &&serial) 
 // n_cycles complete CA cycles (start, grow/claim, capture) in one cooperative launch.
 template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 2) k_cycles(PoolState *P, int n_cycles) {
     CycleStats st;
-    bool ok = grid_meet(P, 0, [&] { begin_cycle(P); });
+    // with many domains, their per-cycle start (termination, nucleation) runs across the grid
+    const bool spread = P->n_domains > kSerialDomains;
+    const int gwarp = (threadIdx.x >> 5) * gridDim.x + blockIdx.x, nwarp = gridDim.x * (kBlock / 32);
+    bool ok = grid_meet(P, 0, [&] {
+        if (spread)
+            begin_lists(P);
+        else
+            begin_cycle(P);
+    });
+    if (ok && spread) {
+        begin_domains(P, gwarp, nwarp);
+        ok = grid_meet(P, -1, [] {});
+    }
     for (int c = 0; ok && c < n_cycles; c++) {
         grow_pass<kBatch>(P, st);
         ok = grid_meet(P, 3 * c + 1, [] {});
@@ -1204,9 +1227,17 @@ template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 2) k
         const bool more = c + 1 < n_cycles;
         ok = grid_meet(P, 3 * c + 3, [&] {
             finish_capture(P);
-            if (more)
-                begin_cycle(P);
+            if (more) {
+                if (spread)
+                    begin_lists(P);
+                else
+                    begin_cycle(P);
+            }
         });
+        if (ok && more && spread) {
+            begin_domains(P, gwarp, nwarp);
+            ok = grid_meet(P, -1, [] {});
+        }
     }
     flush_stats(P, st);
 }
