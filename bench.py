@@ -297,7 +297,7 @@ def b200_arm(args, rank, world, local):
     if os.path.exists(traffic_file):
         for ln in open(traffic_file):
             if ln.startswith("k_cycles "):
-                traffic = float(ln.split()[1]) * args.profile_cycles  # file holds bytes per cycle
+                traffic = float(ln.split()[1]) * args.profile_cycles  # the file holds DRAM bytes per cycle
 
     # dense-equivalent effective roofline (the reference formulation's compulsory bytes per cycle)
     eff_bytes_per_update = 14.5
