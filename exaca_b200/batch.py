@@ -39,6 +39,24 @@ def process_map(n_domains: int = 256, seed: int = 3, side=(32, 128), G=(1e5, 5e6
     return out
 
 
+def footprint(p: dict) -> int:
+    """Device bytes of a domain of these parameters (cells including the wall ring x the per-cell
+    fields of a pool slot); the ranking that partitions a map over GPUs."""
+    return (p["nx"] + 2) * (p["ny"] + 2) * (p["nz"] + 2) * 146
+
+
+def partition(weights: list[int], n_parts: int) -> list[list[int]]:
+    """Greedy bin-packing: items in decreasing weight, each to the currently lightest part (ties to
+    the lowest part index). Deterministic, so every rank computes the same split without talking."""
+    parts = [[] for _ in range(n_parts)]
+    load = [0] * n_parts
+    for i in sorted(range(len(weights)), key=lambda k: (-weights[k], k)):
+        j = min(range(n_parts), key=lambda q: (load[q], q))
+        parts[j].append(i)
+        load[j] += weights[i]
+    return [sorted(p) for p in parts]
+
+
 def build_problems(params: list[dict], threads: int | None = None) -> list[Problem]:
     """Host initialisation of every domain (independent, so it runs on a thread pool)."""
     threads = threads or os.cpu_count() or 1
