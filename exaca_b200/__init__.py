@@ -93,6 +93,13 @@ class CellFieldsT(ctypes.Structure):
 CENSUS_MAX_DOMAINS = 256
 STEP_CONFIGS = 8
 
+class GrainStatsT(ctypes.Structure):
+    _fields_ = [("region_cells", ctypes.c_int64), ("melted_cells", ctypes.c_int64), ("n_grains", ctypes.c_int64),
+                ("mean_grain_volume_um3", ctypes.c_double), ("nucleated_fraction", ctypes.c_double),
+                ("mean_misorientation_deg", ctypes.c_double), ("mean_misorientation_top_deg", ctypes.c_double),
+                ("misorientation_hist", ctypes.c_uint64 * 64)]
+
+
 # Every symbol include/exaca_b200.h declares, with its ctypes signature.
 _P = ctypes.c_void_p
 _I = ctypes.c_int
@@ -124,6 +131,7 @@ SIGNATURES = {
     "exaca_pool_profile_persistent": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_pool_run_all": ([_P, _I, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)], _I),
     "exaca_pool_status_many": ([_P, _I, ctypes.POINTER(_I), ctypes.POINTER(DomainStatus)], _I),
+    "exaca_pool_grain_stats": ([_P, _I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(GrainStatsT)], _I),
     "exaca_pool_set_config": ([_P, _I], _I),
     "exaca_pool_autotune": ([_P, _I, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_problem_pin": ([_P], _I),
@@ -265,6 +273,16 @@ class Pool:
         s = DomainStatus()
         _check(load_library().exaca_pool_status(self._h, slot, ctypes.byref(s)))
         return Status(s.cycle, bool(s.done), s.nn, s.error, s.liquid)
+
+    def grain_stats(self, slot: int, region=None) -> dict:
+        """Grain statistics of the reference analysis for a slot, computed on the device; region =
+        (xmin, xmax, ymin, ymax, zmin, zmax) in .vtk coordinates, None for the interior."""
+        out = GrainStatsT()
+        reg = None if region is None else (ctypes.c_int32 * 6)(*region)
+        _check(load_library().exaca_pool_grain_stats(self._h, slot, reg, ctypes.byref(out)))
+        d = {k: getattr(out, k) for k, _ in GrainStatsT._fields_ if k != "misorientation_hist"}
+        d["misorientation_hist"] = list(out.misorientation_hist)
+        return d
 
     def status_many(self, slots) -> list:
         """status() of several slots with one device read."""

@@ -251,6 +251,30 @@ int exaca_pool_status_many(exaca_pool *pool, int n_slots, const int *slots, exac
     });
 }
 
+int exaca_pool_grain_stats(exaca_pool *pool, int slot, const int32_t *region, exaca_grain_stats *out) {
+    if (!pool || !out || !pool->pool->slot_used(slot))
+        return fail(EXACA_ERR_ARG, "bad slot or null argument");
+    try {
+        exaca::GrainStats g = pool->pool->grain_stats(slot, region);
+        out->region_cells = g.region_cells;
+        out->melted_cells = g.melted_cells;
+        out->n_grains = g.n_grains;
+        out->mean_grain_volume_um3 = g.deltax * g.deltax * pow(10, 12) * ((double)g.region_cells / (double)g.n_grains);
+        out->nucleated_fraction = (double)g.nucleated_cells / (double)g.region_cells;
+        out->mean_misorientation_deg = g.melted_cells ? g.misorientation_sum / (double)g.melted_cells : 0.0;
+        out->mean_misorientation_top_deg = g.top_melted ? g.misorientation_top_sum / (double)g.top_melted : 0.0;
+        for (int b = 0; b < exaca::kMisorientationBins; b++)
+            out->misorientation_hist[b] = g.hist[b];
+        return EXACA_OK;
+    }
+    catch (const std::invalid_argument &e) {
+        return fail(EXACA_ERR_ARG, e.what());
+    }
+    catch (const std::exception &e) {
+        return fail(EXACA_ERR_CUDA, e.what());
+    }
+}
+
 int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st) {
     if (!pool || !st)
         return fail(EXACA_ERR_ARG, "null argument");

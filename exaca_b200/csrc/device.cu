@@ -28,6 +28,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cmath>
 #include <climits>
 #include <cstdio>
 #include <cstdlib>
@@ -2212,6 +2213,205 @@ int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_
         *capture_s = secs;
     slots_[slot].finished = true;
     return cycle;
+}
+
+// ---------------------------------------------------------------------------------------------
+// Grain statistics (analysis/src/GAprint.cpp:17-198) on the device: per region cell, melted count,
+// misorientation of its grain's orientation to +Z (table built on the host with the reference's
+// libm acos), its 1-degree histogram, nucleated cells, GrainID range; then distinct GrainIDs via a
+// bitmap over that range.
+struct GrainAcc {
+    unsigned long long melted, nucleated, top_melted;
+    double mis, mis_top;
+    unsigned long long hist[kMisorientationBins];
+    int gmin, gmax;
+};
+
+struct Region {
+    int x0, x1, y0, y1, z0, z1, mx, my;
+    __device__ __forceinline__ long long count() const {
+        return (long long)(x1 - x0 + 1) * (y1 - y0 + 1) * (z1 - z0 + 1);
+    }
+    // q-th region cell: (k, i, j) of the .vtk grid -> rank-local index (ghost ring offset 1)
+    __device__ __forceinline__ long long cell(long long q, int &k) const {
+        const long long ny_r = y1 - y0 + 1, nx_r = x1 - x0 + 1;
+        const long long j = q % ny_r, t = q / ny_r;
+        const long long i = t % nx_r;
+        k = (int)(t / nx_r) + z0;
+        return (long long)k * mx * my + (i + x0 + 1) * my + (j + y0 + 1);
+    }
+};
+
+__global__ void __launch_bounds__(kBlock) k_grain_region(const int32_t *gid, const int8_t *melted, const float *mis,
+                                                         Region R, GrainAcc *acc) {
+    __shared__ unsigned long long s_hist[kMisorientationBins];
+    for (int b = threadIdx.x; b < kMisorientationBins; b += blockDim.x)
+        s_hist[b] = 0;
+    __syncthreads();
+    unsigned long long m = 0, nuc = 0, top = 0;
+    double ms = 0, mt = 0;
+    int gmin = INT_MAX, gmax = INT_MIN;
+    const long long n = R.count();
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        int k;
+        const long long c = R.cell(q, k);
+        const int g = gid[c];
+        gmin = min(gmin, g);
+        gmax = max(gmax, g);
+        if (g < 0)
+            nuc++;
+        if (melted[c] == 1) {
+            int ori = (abs(g) - 1) % 10000;
+            if (ori < 0)
+                ori += 10000;
+            const float a = mis[ori];
+            m++;
+            ms += a;
+            atomicAdd(&s_hist[min((int)a, kMisorientationBins - 1)], 1ull);
+            if (k == R.z1) {
+                top++;
+                mt += a;
+            }
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        m += __shfl_down_sync(0xffffffffu, m, o);
+        nuc += __shfl_down_sync(0xffffffffu, nuc, o);
+        top += __shfl_down_sync(0xffffffffu, top, o);
+        ms += __shfl_down_sync(0xffffffffu, ms, o);
+        mt += __shfl_down_sync(0xffffffffu, mt, o);
+        gmin = min(gmin, __shfl_down_sync(0xffffffffu, gmin, o));
+        gmax = max(gmax, __shfl_down_sync(0xffffffffu, gmax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (m)
+            atomicAdd(&acc->melted, m);
+        if (nuc)
+            atomicAdd(&acc->nucleated, nuc);
+        if (top)
+            atomicAdd(&acc->top_melted, top);
+        if (ms != 0)
+            atomicAdd(&acc->mis, ms);
+        if (mt != 0)
+            atomicAdd(&acc->mis_top, mt);
+        atomicMin(&acc->gmin, gmin);
+        atomicMax(&acc->gmax, gmax);
+    }
+    __syncthreads();
+    for (int b = threadIdx.x; b < kMisorientationBins; b += blockDim.x)
+        if (s_hist[b])
+            atomicAdd(&acc->hist[b], s_hist[b]);
+}
+
+__global__ void k_grain_bits(const int32_t *gid, Region R, int gmin, unsigned long long *bits) {
+    const long long n = R.count();
+    for (long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x; q < n; q += (long long)gridDim.x * blockDim.x) {
+        int k;
+        const long long off = (long long)gid[R.cell(q, k)] - gmin;
+        atomicOr(bits + (off >> 6), 1ull << (off & 63));
+    }
+}
+
+__global__ void k_popcount(const unsigned long long *bits, long long nwords, unsigned long long *count) {
+    unsigned long long c = 0;
+    for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < nwords; w += (long long)gridDim.x * blockDim.x)
+        c += __popcll(bits[w]);
+    for (int o = 16; o; o >>= 1)
+        c += __shfl_down_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c)
+        atomicAdd(count, c);
+}
+
+GrainStats Pool::grain_stats(int slot, const int *region) {
+    CUDA_OK(cudaSetDevice(device_));
+    if (!slot_used(slot))
+        throw std::invalid_argument("bad slot");
+    const Problem &p = *slots_[slot].problem;
+    const Geometry &g = p.g;
+    Region R;
+    if (region) {
+        R.x0 = region[0], R.x1 = region[1], R.y0 = region[2], R.y1 = region[3], R.z0 = region[4], R.z1 = region[5];
+    }
+    else {
+        R.x0 = 1, R.x1 = g.nx - 2, R.y0 = 1, R.y1 = g.ny - 2, R.z0 = 1, R.z1 = g.nz - 2;
+    }
+    if (R.x0 < 0 || R.x1 >= g.nx || R.y0 < 0 || R.y1 >= g.ny || R.z0 < 0 || R.z1 >= g.nz || R.x0 > R.x1 ||
+        R.y0 > R.y1 || R.z0 > R.z1)
+        throw std::invalid_argument("region outside the domain");
+    R.mx = g.mx;
+    R.my = g.my;
+    // per-orientation misorientation to +Z with the reference's expression (GAprint.cpp:38-46)
+    std::vector<float> mis(kNumOrientations);
+    for (int n = 0; n < kNumOrientations; n++) {
+        double amin = 62.7;
+        for (int ll = 0; ll < 3; ll++) {
+            // double acos of the float component, as the reference's unqualified call on a float
+            double a = std::abs((180 / M_PI) * std::acos((double)p.guv[9 * n + 3 * ll + 2]));
+            if (a < amin)
+                amin = a;
+        }
+        mis[n] = (float)amin;
+    }
+    cudaStream_t st = S(stream_);
+    const size_t N = g.domain_size;
+    int8_t *dmel = nullptr;
+    float *dmis = nullptr;
+    GrainAcc *dacc = nullptr;
+    unsigned long long *bits = nullptr, *dcount = nullptr;
+    GrainStats out;
+    try {
+        CUDA_OK(cudaMalloc(&dmel, N));
+        CUDA_OK(cudaMalloc(&dmis, mis.size() * sizeof(float)));
+        CUDA_OK(cudaMalloc(&dacc, sizeof(GrainAcc)));
+        CUDA_OK(cudaMalloc(&dcount, sizeof(unsigned long long)));
+        GrainAcc init;
+        std::memset(&init, 0, sizeof(init));
+        init.gmin = INT_MAX;
+        init.gmax = INT_MIN;
+        CUDA_OK(cudaMemcpyAsync(dmel, p.melted.data(), N, cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(dmis, mis.data(), mis.size() * sizeof(float), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(dacc, &init, sizeof(init), cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemsetAsync(dcount, 0, sizeof(unsigned long long), st));
+        k_grain_region<<<num_sms_ * 4, kBlock, 0, st>>>(host_desc_[slot].gid, dmel, dmis, R, dacc);
+        CUDA_OK(cudaGetLastError());
+        GrainAcc acc;
+        CUDA_OK(cudaMemcpyAsync(&acc, dacc, sizeof(acc), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        const long long range = (long long)acc.gmax - acc.gmin + 1;
+        const long long nwords = (range + 63) / 64;
+        CUDA_OK(cudaMalloc(&bits, nwords * 8));
+        CUDA_OK(cudaMemsetAsync(bits, 0, nwords * 8, st));
+        k_grain_bits<<<num_sms_ * 4, kBlock, 0, st>>>(host_desc_[slot].gid, R, acc.gmin, bits);
+        k_popcount<<<num_sms_ * 2, kBlock, 0, st>>>(bits, nwords, dcount);
+        CUDA_OK(cudaGetLastError());
+        unsigned long long count = 0;
+        CUDA_OK(cudaMemcpyAsync(&count, dcount, sizeof(count), cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaStreamSynchronize(st));
+        out.region_cells = (long long)(R.x1 - R.x0 + 1) * (R.y1 - R.y0 + 1) * (R.z1 - R.z0 + 1);
+        out.melted_cells = (long long)acc.melted;
+        out.nucleated_cells = (long long)acc.nucleated;
+        out.top_melted = (long long)acc.top_melted;
+        out.n_grains = (long long)count;
+        out.misorientation_sum = acc.mis;
+        out.misorientation_top_sum = acc.mis_top;
+        out.deltax = p.cfg.deltax;
+        for (int b = 0; b < kMisorientationBins; b++)
+            out.hist[b] = acc.hist[b];
+    }
+    catch (...) {
+        cudaFree(dmel);
+        cudaFree(dmis);
+        cudaFree(dacc);
+        cudaFree(bits);
+        cudaFree(dcount);
+        throw;
+    }
+    cudaFree(dmel);
+    cudaFree(dmis);
+    cudaFree(dacc);
+    cudaFree(bits);
+    cudaFree(dcount);
+    return out;
 }
 
 } // namespace exaca

@@ -153,6 +153,14 @@ struct Census {
     unsigned long long next_cts; // min CritTimeStep of liquid cells in the active window
 };
 
+// Grain statistics of the reference analysis (analysis/src/GAprint.cpp:17-198) over one region.
+constexpr int kMisorientationBins = 64;
+struct GrainStats {
+    long long region_cells = 0, melted_cells = 0, n_grains = 0, nucleated_cells = 0, top_melted = 0;
+    double misorientation_sum = 0, misorientation_top_sum = 0, deltax = 0;
+    unsigned long long hist[kMisorientationBins] = {};
+};
+
 struct DeviceTables {
     float *guv = nullptr;
     float *cdl_table = nullptr;
@@ -201,6 +209,9 @@ class Pool {
     double last_run_ms() const { return last_run_ms_; }
     // runs n cycles as separate per-pass kernels with CUDA events around each launch
     KernelTimes profile_cycles(int n);
+    // Grain statistics of a slot's GrainID field over a region in .vtk coordinates
+    // {xmin, xmax, ymin, ymax, zmin, zmax} (null: the interior without wall layers).
+    GrainStats grain_stats(int slot, const int *region);
     // step(n) with CUDA events around the launches; returns their device time in ms
     double timed_step(int n);
     // Step configurations: config = mode * kStepVariants + variant. set_config switches; autotune

@@ -166,6 +166,23 @@ int exaca_pool_copy_octahedra(exaca_pool *pool, int slot, float *dl, float *doc,
 int exaca_pool_retire(exaca_pool *pool, int slot);
 int64_t exaca_pool_bytes_in_use(exaca_pool *pool);
 
+/* Grain statistics of the reference analysis (analysis/src/GAprint.cpp:17-198: PrintMisorientationData,
+ * PrintSizeData) computed on the device from a slot's GrainID field, without writing .vtk files. */
+#define EXACA_MISORIENTATION_BINS 64
+typedef struct {
+    int64_t region_cells;               /* cells in the region */
+    int64_t melted_cells;               /* region cells that melted */
+    int64_t n_grains;                   /* distinct GrainIDs in the region */
+    double mean_grain_volume_um3;       /* the reference's expression: deltax^2 * 1e12 * cells / grains */
+    double nucleated_fraction;          /* region cells with a nucleated (negative) GrainID */
+    double mean_misorientation_deg;     /* mean over melted cells of the grain's smallest angle to +Z */
+    double mean_misorientation_top_deg; /* the same over the region's top plane */
+    uint64_t misorientation_hist[EXACA_MISORIENTATION_BINS]; /* melted cells per 1-degree bin (last: >= 63) */
+} exaca_grain_stats;
+/* region: {xmin, xmax, ymin, ymax, zmin, zmax} in the coordinates of the .vtk output (whole domain
+ * with walls, no ghost ring), or NULL for the interior without the wall layers. */
+int exaca_pool_grain_stats(exaca_pool *pool, int slot, const int32_t *region, exaca_grain_stats *out);
+
 /* Writes the reference's output files for a finished slot (src/CAprint.cpp:170-571). */
 int exaca_pool_write_outputs(exaca_pool *pool, int slot, const exaca_problem *p, const char *path_prefix);
 
