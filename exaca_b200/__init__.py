@@ -125,6 +125,7 @@ SIGNATURES = {
     "exaca_pool_retire": ([_P, _I], _I),
     "exaca_pool_bytes_in_use": ([_P], ctypes.c_int64),
     "exaca_pool_write_outputs": ([_P, _I, _P, ctypes.c_char_p], _I),
+    "exaca_problem_write_outputs": ([_P, _P, ctypes.c_char_p, _I], _I),
     "exaca_pool_last_run_ms": ([_P], ctypes.c_double),
     "exaca_pool_profile_cycles": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_pool_timed_step": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
@@ -232,6 +233,14 @@ class Problem:
 
     def slot_bytes(self) -> int:
         return int(load_library().exaca_problem_slot_bytes(self._h))
+
+    def write_outputs(self, grain_id: np.ndarray, prefix: str, threads: int = 0) -> None:
+        """The .vtk / _Misorientations.vtk files the problem's print flags ask for, from a host GrainID
+        (the layout of Pool.copy_out), formatted on `threads` host threads (0: all)."""
+        gid = np.ascontiguousarray(grain_id, dtype=np.int32)
+        if gid.size != self.geometry.domain_size:
+            raise ValueError(f"GrainID has {gid.size} cells, the problem {self.geometry.domain_size}")
+        _check(load_library().exaca_problem_write_outputs(self._h, _ptr(gid), os.fsencode(prefix), int(threads)))
 
     def pin(self) -> None:
         """Page-locks the host fields so admission copies run at full PCIe bandwidth."""

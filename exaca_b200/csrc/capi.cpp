@@ -70,18 +70,19 @@ void emit(std::string &log) {
     log.clear();
 }
 
-void write_outputs(const exaca::Problem &p, const int32_t *gid, const std::string &prefix, std::string &log) {
+void write_outputs(const exaca::Problem &p, const int32_t *gid, const std::string &prefix, std::string &log,
+                   int threads = 0) {
     const exaca::InputConfig &c = p.cfg;
     if (c.print_misorientation || c.print_full_output) {
         log += "Collecting data on rank 0 and printing to files\n";
         if (c.print_misorientation) {
             log += "Printing Paraview file of grain misorientations\n";
-            exaca::write_misorientations(p, gid, prefix + "_Misorientations.vtk", log);
+            exaca::write_misorientations(p, gid, prefix + "_Misorientations.vtk", log, threads);
         }
         if (c.print_full_output) {
             log += "Printing layer ID, grain ID, and melted 0/1 data to a vtk file " + prefix +
                    ".vtk for post-processing\n";
-            exaca::write_vtk_fields(p, gid, prefix + ".vtk");
+            exaca::write_vtk_fields(p, gid, prefix + ".vtk", threads);
         }
     }
     else {
@@ -440,6 +441,16 @@ int exaca_pool_write_outputs(exaca_pool *pool, int slot, const exaca_problem *p,
         std::string out;
         exaca::RunTimes t;
         exaca::write_log(*p->p, std::string(path_prefix) + ".log", pool->pool->state(slot).cycle, t, out);
+    });
+}
+
+int exaca_problem_write_outputs(const exaca_problem *p, const int32_t *grain_id, const char *path_prefix,
+                                int threads) {
+    if (!p || !grain_id || !path_prefix)
+        return fail(EXACA_ERR_ARG, "bad argument");
+    return guarded([&] {
+        std::string log;
+        write_outputs(*p->p, grain_id, path_prefix, log, threads);
     });
 }
 

@@ -137,10 +137,12 @@ void unpin_problem(Problem &p);
 void read_orientations(const std::string &path, std::vector<float> &guv);
 void build_cdl_table(const std::vector<float> &guv, std::vector<float> &table);
 
-// Output writers (src/CAprint.cpp:170-571), byte-compatible with the reference.
-void write_vtk_fields(const Problem &p, const int32_t *grain_id, const std::string &fname);
+// Output writers (src/CAprint.cpp:170-571), byte-compatible with the reference. `threads` host
+// threads format the z planes (<= 0: $EXACA_OUTPUT_THREADS, else every hardware thread); the
+// bytes do not depend on it.
+void write_vtk_fields(const Problem &p, const int32_t *grain_id, const std::string &fname, int threads = 0);
 void write_misorientations(const Problem &p, const int32_t *grain_id, const std::string &fname,
-                           std::string &log);
+                           std::string &log, int threads = 0);
 void write_debug_vtk(const Problem &p, const std::string &fname);
 
 struct RunTimes {

@@ -1,37 +1,42 @@
 // Output writers of the B200 solver: the ASCII legacy-VTK field file, the misorientation file, the
 // init debug file and the run log. The byte layout is the reference's (src/CAprint.cpp:285-571):
 // same headers, same (k, j, i) value order with x fastest, one line per z plane, every value
-// followed by a space. Values are formatted with a buffered integer formatter instead of
-// iostreams, which gives identical text for ints.
+// followed by a space. Values are formatted with an integer digit loop instead of iostreams (the
+// same text for ints), one z plane per task on all host threads, and written in plane order.
 #include "exaca_host.hpp"
 
+#include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <fstream>
+#include <mutex>
 #include <sstream>
+#include <thread>
 
 namespace exaca {
 
 namespace {
 
-class TextOut {
+// Text of one z plane, built with plain appends (ints by a digit loop; floats by "%f", which is
+// what `std::fixed` iostream output prints). One cache line each: threads append to neighbouring
+// planes at the same time.
+class alignas(64) PlaneText {
   public:
-    explicit TextOut(const std::string &fname) : f_(std::fopen(fname.c_str(), "wb")) {
-        if (!f_)
-            throw std::runtime_error("could not open output file " + fname);
-        buf_.resize(1 << 22);
+    void clear() { n_ = 0; }
+    void reserve(size_t bytes) {
+        if (buf_.size() < bytes)
+            buf_.resize(bytes);
     }
-    ~TextOut() {
-        flush();
-        if (f_)
-            std::fclose(f_);
-    }
-    void put(const std::string &s) {
-        for (char c : s)
-            putc_(c);
+    void put(const char *s, size_t len) {
+        need(len);
+        std::memcpy(buf_.data() + n_, s, len);
+        n_ += len;
     }
     void put_int(long v) {
+        need(24);
         char tmp[24];
         int n = 0;
         bool neg = v < 0;
@@ -41,32 +46,116 @@ class TextOut {
             u /= 10;
         } while (u);
         if (neg)
-            putc_('-');
+            buf_[n_++] = '-';
         while (n)
-            putc_(tmp[--n]);
+            buf_[n_++] = tmp[--n];
     }
     void put_fixed(float v) {
-        char tmp[64];
-        int n = std::snprintf(tmp, sizeof(tmp), "%f", (double)v);
-        for (int i = 0; i < n; i++)
-            putc_(tmp[i]);
+        need(64);
+        n_ += (size_t)std::snprintf(buf_.data() + n_, 64, "%f", (double)v);
     }
     void putc_(char c) {
-        if (pos_ == buf_.size())
-            flush();
-        buf_[pos_++] = c;
+        need(1);
+        buf_[n_++] = c;
     }
-    void flush() {
-        if (pos_ && f_)
-            std::fwrite(buf_.data(), 1, pos_, f_);
-        pos_ = 0;
+    const char *data() const { return buf_.data(); }
+    size_t size() const { return n_; }
+
+  private:
+    void need(size_t len) {
+        if (n_ + len > buf_.size())
+            buf_.resize(std::max(buf_.size() * 2, n_ + len + 4096));
+    }
+    std::vector<char> buf_;
+    size_t n_ = 0;
+};
+
+class File {
+  public:
+    explicit File(const std::string &fname) : f_(std::fopen(fname.c_str(), "wb")) {
+        if (!f_)
+            throw std::runtime_error("could not open output file " + fname);
+    }
+    ~File() {
+        if (f_)
+            std::fclose(f_);
+    }
+    void put(const std::string &s) { write(s.data(), s.size()); }
+    void write(const char *p, size_t n) {
+        if (n && std::fwrite(p, 1, n, f_) != n)
+            throw std::runtime_error("write to output file failed");
     }
 
   private:
     std::FILE *f_;
-    std::vector<char> buf_;
-    size_t pos_ = 0;
 };
+
+int output_threads() {
+    if (const char *e = std::getenv("EXACA_OUTPUT_THREADS")) {
+        int t = std::atoi(e);
+        if (t > 0)
+            return t;
+    }
+    unsigned hc = std::thread::hardware_concurrency();
+    return hc ? (int)hc : 1;
+}
+
+// Formats planes 0..n-1 with `plane(k, text)` on `threads` host threads, a batch of planes at a
+// time (bounded memory), and writes them to `f` in plane order; the writes of one batch overlap
+// the formatting of the next. The bytes are those of formatting the planes one after another.
+template <class Fn> void write_planes(File &f, int n, int threads, size_t plane_bytes, Fn &&plane) {
+    threads = std::max(1, std::min(threads, n));
+    const int batch = threads * 4;
+    std::vector<PlaneText> sets[2] = {std::vector<PlaneText>(batch), std::vector<PlaneText>(batch)};
+    std::thread writer;
+    std::exception_ptr werr;
+    int s = 0;
+    for (int b = 0; b < n; b += batch) {
+        const int m = std::min(batch, n - b);
+        std::vector<PlaneText> &set = sets[s];
+        std::atomic<int> next{0};
+        std::exception_ptr ferr;
+        std::mutex ferr_mu;
+        auto work = [&] {
+            try {
+                for (int i; (i = next.fetch_add(1)) < m;) {
+                    set[i].clear();
+                    set[i].reserve(plane_bytes);
+                    plane(b + i, set[i]);
+                }
+            } catch (...) {
+                std::lock_guard<std::mutex> lk(ferr_mu);
+                ferr = std::current_exception();
+            }
+        };
+        std::vector<std::thread> pool;
+        for (int t = 1; t < std::min(threads, m); t++)
+            pool.emplace_back(work);
+        work();
+        for (auto &t : pool)
+            t.join();
+        if (writer.joinable())
+            writer.join();
+        if (ferr)
+            std::rethrow_exception(ferr);
+        if (werr)
+            std::rethrow_exception(werr);
+        std::vector<PlaneText> *done = &set;
+        writer = std::thread([&f, done, m, &werr] {
+            try {
+                for (int i = 0; i < m; i++)
+                    f.write((*done)[i].data(), (*done)[i].size());
+            } catch (...) {
+                werr = std::current_exception();
+            }
+        });
+        s ^= 1;
+    }
+    if (writer.joinable())
+        writer.join();
+    if (werr)
+        std::rethrow_exception(werr);
+}
 
 // Whole-domain view of a rank-local field without the ghost ring: value at (k, x, y) for
 // x in [0, nx), y in [0, ny); planes k = 0 and k = nz - 1 read as zero (src/CAprint.cpp:18-29,
@@ -77,78 +166,84 @@ template <class T> long whole(const Geometry &g, const T *f, int k, int x, int y
     return (long)f[(long)k * g.mx * g.my + (long)(x + 1) * g.my + (y + 1)];
 }
 
-void vtk_header(TextOut &o, int nx, int ny, int nz) {
+void vtk_header(File &o, int nx, int ny, int nz) {
     o.put("# vtk DataFile Version 3.0\nvtk output\nASCII\nDATASET STRUCTURED_POINTS\n");
     o.put("DIMENSIONS " + std::to_string(nx) + " " + std::to_string(ny) + " " + std::to_string(nz) + "\n");
     o.put("ORIGIN 0 0 0\nSPACING 1 1 1\n");
-    o.put("POINT_DATA " + std::to_string(nx * ny * nz) + "\n");
+    o.put("POINT_DATA " + std::to_string((long)nx * ny * nz) + "\n");
 }
 
-template <class T> void int_block(TextOut &o, const Geometry &g, const char *name, const T *f) {
+template <class T> void int_block(File &o, const Geometry &g, const char *name, const T *f, int threads) {
     o.put(std::string("SCALARS ") + name + " int 1\nLOOKUP_TABLE default\n");
-    for (int k = 0; k < g.nz; k++) {
+    write_planes(o, g.nz, threads, (size_t)g.nx * g.ny * 4 + 64, [&](int k, PlaneText &t) {
         for (int j = 0; j < g.ny; j++)
             for (int i = 0; i < g.nx; i++) {
-                o.put_int(whole(g, f, k, i, j));
-                o.putc_(' ');
+                t.put_int(whole(g, f, k, i, j));
+                t.putc_(' ');
             }
-        o.putc_('\n');
-    }
+        t.putc_('\n');
+    });
 }
 
-void float_block(TextOut &o, const Geometry &g, const char *name, const float *f) {
+void float_block(File &o, const Geometry &g, const char *name, const float *f, int threads) {
     o.put(std::string("SCALARS ") + name + " float 1\nLOOKUP_TABLE default\n");
-    for (int k = 0; k < g.nz; k++) {
+    write_planes(o, g.nz, threads, (size_t)g.nx * g.ny * 10 + 64, [&](int k, PlaneText &t) {
         for (int j = 0; j < g.ny; j++)
             for (int i = 0; i < g.nx; i++) {
                 float v = (k == 0 || k == g.nz - 1) ? 0.0f : f[(long)k * g.mx * g.my + (long)(i + 1) * g.my + (j + 1)];
-                o.put_fixed(v);
-                o.putc_(' ');
+                t.put_fixed(v);
+                t.putc_(' ');
             }
-        o.putc_('\n');
-    }
+        t.putc_('\n');
+    });
 }
 
 } // namespace
 
-void write_vtk_fields(const Problem &p, const int32_t *grain_id, const std::string &fname) {
+void write_vtk_fields(const Problem &p, const int32_t *grain_id, const std::string &fname, int threads) {
     // src/CAprint.cpp:285-346 with PrintFullOutput: LayerID, GrainID, Melted
-    TextOut o(fname);
+    if (threads <= 0)
+        threads = output_threads();
+    File o(fname);
     const Geometry &g = p.g;
     vtk_header(o, g.nx, g.ny, g.nz);
-    int_block(o, g, "LayerID", p.layer_id.data());
-    int_block(o, g, "GrainID", grain_id);
-    int_block(o, g, "Melted", p.melted.data());
+    int_block(o, g, "LayerID", p.layer_id.data(), threads);
+    int_block(o, g, "GrainID", grain_id, threads);
+    int_block(o, g, "Melted", p.melted.data(), threads);
 }
 
 void write_debug_vtk(const Problem &p, const std::string &fname) {
     // src/CAprint.cpp:285-395 with PrintFullOutput false: the init debug dump of PrintDebug 1 or 2
-    TextOut o(fname);
+    const int threads = output_threads();
+    File o(fname);
     const Geometry &g = p.g;
     vtk_header(o, g.nx, g.ny, g.nz);
-    int_block(o, g, "LayerID", p.layer_id.data());
+    int_block(o, g, "LayerID", p.layer_id.data(), threads);
     if (p.cfg.print_debug == 2) {
-        int_block(o, g, "GrainID", p.grain_id.data());
-        int_block(o, g, "Melted", p.melted.data());
+        int_block(o, g, "GrainID", p.grain_id.data(), threads);
+        int_block(o, g, "Melted", p.melted.data(), threads);
     }
-    int_block(o, g, "CritTimeStep", p.cts.data());
-    int_block(o, g, "CellType", p.cell_type.data());
+    int_block(o, g, "CritTimeStep", p.cts.data(), threads);
+    int_block(o, g, "CellType", p.cell_type.data(), threads);
     if (p.cfg.print_debug == 2) {
-        float_block(o, g, "UndercoolingChange", p.du.data());
+        float_block(o, g, "UndercoolingChange", p.du.data(), threads);
         std::vector<float> zeros(g.domain_size, 0.0f); // UndercoolingCurrent is 0 after init
-        float_block(o, g, "Melted", zeros.data());
+        float_block(o, g, "Melted", zeros.data(), threads);
     }
 }
 
-void write_misorientations(const Problem &p, const int32_t *grain_id, const std::string &fname, std::string &log) {
+void write_misorientations(const Problem &p, const int32_t *grain_id, const std::string &fname, std::string &log,
+                           int threads) {
     // src/CAprint.cpp:398-460
+    if (threads <= 0)
+        threads = output_threads();
     const Geometry &g = p.g;
-    TextOut o(fname);
+    File o(fname);
     o.put("# vtk DataFile Version 3.0\nvtk output\nASCII\nDATASET STRUCTURED_POINTS\n");
     o.put("DIMENSIONS " + std::to_string(g.nx - 2) + " " + std::to_string(g.ny - 2) + " " +
           std::to_string(g.nz - 2) + "\n");
     o.put("ORIGIN 0 0 0\nSPACING 1 1 1\n");
-    o.put("POINT_DATA " + std::to_string((g.nx - 2) * (g.ny - 2) * (g.nz - 2)) + "\n");
+    o.put("POINT_DATA " + std::to_string((long)(g.nx - 2) * (g.ny - 2) * (g.nz - 2)) + "\n");
     o.put("SCALARS Angle_z int 1\nLOOKUP_TABLE default\n");
     std::vector<int> rounded(kNumOrientations);
     for (int n = 0; n < kNumOrientations; n++) {
@@ -160,16 +255,19 @@ void write_misorientations(const Problem &p, const int32_t *grain_id, const std:
         }
         rounded[n] = round(amin);
     }
-    int nucleated = 0, melted = 0;
-    for (int k = 1; k < g.nz - 1; k++) {
+    // per-plane counts, summed afterwards (the order of integer sums does not matter)
+    std::vector<long> nucleated(g.nz, 0), melted(g.nz, 0);
+    write_planes(o, g.nz - 2, threads, (size_t)g.nx * g.ny * 4 + 64, [&](int kk, PlaneText &t) {
+        const int k = kk + 1;
+        long nuc = 0, mel = 0;
         for (int j = 1; j < g.ny - 1; j++)
             for (int i = 1; i < g.nx - 1; i++) {
                 long idx = (long)k * g.mx * g.my + (long)(i + 1) * g.my + (j + 1);
                 if (p.melted[idx] == 0) {
-                    o.put("200 ");
+                    t.put("200 ", 4);
                 }
                 else {
-                    melted++;
+                    mel++;
                     int gid = grain_id[idx];
                     int ori = (std::abs(gid) - 1) % kNumOrientations;
                     if (ori < 0)
@@ -177,20 +275,28 @@ void write_misorientations(const Problem &p, const int32_t *grain_id, const std:
                     int angle;
                     if (gid < 0) {
                         angle = rounded[ori] + 100;
-                        nucleated++;
+                        nuc++;
                     }
                     else {
                         angle = rounded[ori];
                     }
-                    o.put_int(angle);
-                    o.putc_(' ');
+                    t.put_int(angle);
+                    t.putc_(' ');
                 }
             }
-        o.putc_('\n');
+        t.putc_('\n');
+        nucleated[k] = nuc;
+        melted[k] = mel;
+    });
+    long n_nuc = 0, n_mel = 0;
+    for (int k = 0; k < g.nz; k++) {
+        n_nuc += nucleated[k];
+        n_mel += melted[k];
     }
+    // the reference counts in int and divides as float
     std::ostringstream s;
     s << "Volume fraction of solidified portion of domain claimed by nucleated grains: "
-      << (float)(nucleated) / (float)(melted) << "\n";
+      << (float)((int)n_nuc) / (float)((int)n_mel) << "\n";
     log += s.str();
 }
 

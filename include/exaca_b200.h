@@ -186,6 +186,16 @@ int exaca_pool_grain_stats(exaca_pool *pool, int slot, const int32_t *region, ex
 /* Writes the reference's output files for a finished slot (src/CAprint.cpp:170-571). */
 int exaca_pool_write_outputs(exaca_pool *pool, int slot, const exaca_problem *p, const char *path_prefix);
 
+/* The .vtk / _Misorientations.vtk files that the problem's print flags ask for
+ * (src/CAprint.cpp:170-460), from a host GrainID in the layout of
+ * exaca_pool_copy_out, without a device. The z planes are formatted on `threads` host threads
+ * (<= 0: $EXACA_OUTPUT_THREADS, else every hardware thread) and written in order; the bytes are
+ * the reference's whatever the thread count. Replaces the rank-0 collect-and-print of
+ * PrintExaCAData (src/CAprint.cpp:170-282): PrintCAFields (:285-395) and
+ * PrintGrainMisorientations (:398-460). */
+int exaca_problem_write_outputs(const exaca_problem *p, const int32_t *grain_id, const char *path_prefix,
+                                int threads);
+
 /* ---- Census without device allocation (no counterpart in the reference) ----
  * The census of IntermediateOutputAndCheck (src/CAupdate.cpp:738-808) computed over cell fields that
  * the caller holds in device memory, for callers that must not allocate device memory: a monitor
