@@ -67,7 +67,8 @@ class DirsParams(ctypes.Structure):
 class DomainStatus(ctypes.Structure):
     _fields_ = [
         ("cycle", ctypes.c_int), ("done", ctypes.c_int), ("nn", ctypes.c_int), ("error", ctypes.c_int),
-        ("liquid", ctypes.c_int64),
+        ("liquid", ctypes.c_int64), ("layer", ctypes.c_int), ("window_z_lo", ctypes.c_int),
+        ("window_nz", ctypes.c_int), ("reserved", ctypes.c_int),
     ]
 
 
@@ -259,6 +260,9 @@ class Status:
     nn: int
     error: int
     liquid: int
+    layer: int = 0
+    window_z_lo: int = 0
+    window_nz: int = 0
 
 
 class Pool:
@@ -281,7 +285,7 @@ class Pool:
     def status(self, slot: int) -> Status:
         s = DomainStatus()
         _check(load_library().exaca_pool_status(self._h, slot, ctypes.byref(s)))
-        return Status(s.cycle, bool(s.done), s.nn, s.error, s.liquid)
+        return Status(s.cycle, bool(s.done), s.nn, s.error, s.liquid, s.layer, s.window_z_lo, s.window_nz)
 
     def grain_stats(self, slot: int, region=None) -> dict:
         """Grain statistics of the reference analysis for a slot, computed on the device; region =
@@ -299,7 +303,8 @@ class Pool:
         arr = (_I * max(n, 1))(*slots)
         out = (DomainStatus * max(n, 1))()
         _check(load_library().exaca_pool_status_many(self._h, n, arr, out))
-        return [Status(s.cycle, bool(s.done), s.nn, s.error, s.liquid) for s in out[:n]]
+        return [Status(s.cycle, bool(s.done), s.nn, s.error, s.liquid, s.layer, s.window_z_lo, s.window_nz)
+                for s in out[:n]]
 
     def stats(self) -> dict:
         s = PoolStatsT()
@@ -324,7 +329,11 @@ class Pool:
         return gid, ct
 
     def copy_octahedra(self, slot: int):
-        a = self._problems[slot].geometry.active_size
+        """Octahedron state of the current layer's active window (DL, DOCenter x3, CDL x26 per cell)."""
+        s = DomainStatus()
+        _check(load_library().exaca_pool_status(self._h, slot, ctypes.byref(s)))
+        g = self._problems[slot].geometry
+        a = g.mx * g.my * s.window_nz
         dl = np.empty(a, np.float32)
         doc = np.empty(3 * a, np.float32)
         cdl = np.empty(26 * a, np.float32)

@@ -229,6 +229,10 @@ int exaca_pool_status(exaca_pool *pool, int slot, exaca_domain_status *st) {
         st->nn = d.nn;
         st->error = d.error | pool->pool->pool_error();
         st->liquid = pool->pool->liquid(slot);
+        st->layer = d.layer_no;
+        st->window_z_lo = d.z_lo;
+        st->window_nz = d.z_end - d.z_lo;
+        st->reserved = 0;
     });
 }
 
@@ -248,6 +252,10 @@ int exaca_pool_status_many(exaca_pool *pool, int n_slots, const int *slots, exac
             st[i].nn = d.nn;
             st[i].error = d.error | perr;
             st[i].liquid = pool->pool->liquid(slots[i]);
+            st[i].layer = d.layer_no;
+            st[i].window_z_lo = d.z_lo;
+            st[i].window_nz = d.z_end - d.z_lo;
+            st[i].reserved = 0;
         }
     });
 }

@@ -192,15 +192,16 @@ __device__ __forceinline__ void cell_coords(const DomainDesc &D, unsigned int c,
     ry = (int)(rem - x * (unsigned int)D.my);
 }
 
-// Edge case of src/CAfunctions.cpp:169-213 as a direction mask, restricted to the active window in
-// z (src/CAupdate.cpp:328 checks MyNeighborZ < nzActive; the lower bound never binds for active
-// cells and is kept as a guard).
+// Edge case of src/CAfunctions.cpp:169-213 as a direction mask, restricted to the top of the active
+// window in z (src/CAupdate.cpp:328 checks MyNeighborZ < nzActive, window-relative; there is no
+// lower check in the reference, which reads one plane below the window; here z >= 0 is kept as a
+// guard).
 __device__ __forceinline__ unsigned int neighbour_mask(const DomainDesc &D, int rx, int ry, int rz) {
     int b = (ry == 0) ? (rx == 0 ? 5 : (rx == D.mx - 1 ? 6 : 1))
                       : (ry == D.my - 1 ? (rx == 0 ? 7 : (rx == D.mx - 1 ? 8 : 2))
                                         : (rx == 0 ? 3 : (rx == D.mx - 1 ? 4 : 0)));
     unsigned int m = c_itmask[b];
-    if (rz + 1 >= D.nz_active)
+    if (rz + 1 >= D.z_end)
         m &= ~c_zplus;
     if (rz - 1 < 0)
         m &= ~c_zminus;
@@ -465,7 +466,7 @@ __device__ __noinline__ void begin_domains(PoolState *P, int first_warp, int war
                 }
                 else {
                     loc = (unsigned int)l;
-                    fire = __ldcg(D.ctype + loc) == kLiquid && D.layer[loc] <= 0;
+                    fire = __ldcg(D.ctype + loc) == kLiquid && D.layer[loc] <= D.layer_no;
                 }
             }
             if (fire) {
@@ -476,7 +477,7 @@ __device__ __noinline__ void begin_domains(PoolState *P, int first_warp, int war
                     r.cell = loc;
                     r.dl = 0.01f;
                     r.cdl_min = 0.0f;
-                    r.cts = D.cts[loc];
+                    r.cts = D.cts_run[loc];
                     P->rec[cur][pos] = r;
                     P->rdom[cur][pos] = (unsigned int)d;
                     P->rstat[cur][pos] = kMaskFresh;
@@ -565,7 +566,7 @@ __device__ __forceinline__ int grow_record(DomainDesc &D, ActiveRec &r, unsigned
         return 0;
     }
     if (!(D.cycle > r.cts))
-        return 1; // single-layer problems only: LayerID <= layer always holds
+        return 1; // cts is INT_MAX outside the window and for LayerID > layer
     st.grown++;
     if (!inc_ok)
         atomicOr(&D.error, kErrGrowthTable);
@@ -590,9 +591,13 @@ __device__ __forceinline__ float effective_min(const ActiveRec &r, unsigned int 
     return (d1 >= 26u || ((m >> d1) & 1u)) ? r.cdl_min : __uint_as_float((unsigned int)min2);
 }
 
-__device__ __forceinline__ void load_growth(const DomainDesc &D, const ActiveRec &r, double &inc, bool &ok) {
-    // undercooling after the executed updates since the liquidus (src/CAupdate.cpp:236-237)
+__device__ __forceinline__ void load_growth(const DomainDesc &D, const ActiveRec &r, double &inc, bool &ok,
+                                            bool multilayer) {
+    // undercooling after the executed updates since the liquidus (src/CAupdate.cpp:236-237), plus
+    // those of earlier layers
     long long nu = executed_upto(D, D.cycle) - executed_upto(D, r.cts);
+    if (multilayer && D.nu_base)
+        nu += __ldg(D.nu_base + r.cell);
     if (D.zero_du && D.du[r.cell] == 0.0f)
         nu = 0;
     ok = nu >= 0 && nu < D.growth_len;
@@ -737,6 +742,7 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
                                          unsigned long long n, CycleStats &st) {
     const unsigned int lane = threadIdx.x & 31;
     DomainDesc *desc = P->desc;
+    const bool multilayer = P->multilayer;
     const ActiveRec *in = P->rec[cur];
     const unsigned int *in_dom = P->rdom[cur];
     const unsigned int *in_stat = P->rstat[cur];
@@ -763,7 +769,7 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
             if (r.cell != kTombstone) {
                 double inc;
                 bool ok;
-                load_growth(desc[dom], r, inc, ok);
+                load_growth(desc[dom], r, inc, ok, multilayer);
                 keep = grow_record(desc[dom], r, m, inc, ok, effective_min(r, m, mn2), st) != 0;
                 if (!keep)
                     st.dropped++;
@@ -803,6 +809,7 @@ template <int kBatch> __device__ void grow_pass(PoolState *P, CycleStats &st) {
     unsigned int *in_stat = P->rstat[cur];
     const unsigned long long *in_min2 = P->rmin2[cur];
     DomainDesc *desc = P->desc;
+    const bool multilayer = P->multilayer;
     unsigned long long tombs = 0;
     const unsigned long long groups = (n + 31) / 32;
     // records are updated in place; dropped ones become tombstones
@@ -838,7 +845,7 @@ template <int kBatch> __device__ void grow_pass(PoolState *P, CycleStats &st) {
                     m[q] &= ~kMaskKeep;
                     in_stat[idx[q]] = m[q];
                 }
-                load_growth(desc[dom[q]], r[q], inc[q], ok[q]);
+                load_growth(desc[dom[q]], r[q], inc[q], ok[q], multilayer);
             }
         }
         unsigned int flagged = 0;
@@ -978,7 +985,7 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         // Every load of the capture and of the re-checks goes out in one round; only the group of
         // the winning claim (the lowest claimant index) continues.
         const unsigned long long key = __ldcg(D.claim + t);
-        const int cts_t = __ldg(D.cts + t);
+        const int cts_t = __ldg(D.cts_run + t);
         const int h = __ldcg(D.gid + c);
         const float docx = __ldcg(D.doc + 3ull * c + 0), docy = __ldcg(D.doc + 3ull * c + 1),
                     docz = __ldcg(D.doc + 3ull * c + 2);
@@ -996,7 +1003,7 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
             a[k] = (unsigned int)((long long)t + (act[k] ? nb_offset(ln, plane, my) : 0));
             ct[k] = __ldcg(D.ctype + a[k]);
             p[k] = __ldcg(D.pos + a[k]);
-            cts_a[k] = __ldg(D.cts + a[k]);
+            cts_a[k] = __ldg(D.cts_run + a[k]);
         }
         if ((unsigned int)key != c) {
             // a lower-index claimant captures t; this claim's slot stays a dropped record
@@ -1259,42 +1266,78 @@ const StepKernels kStepKernel[kStepVariants] = {
     step_kernels<kLaneChoices[1], kBatchChoices[0]>(), step_kernels<kLaneChoices[1], kBatchChoices[1]>()};
 
 // ---------------------------------------------------------------------------------------------
-// Census of src/CAupdate.cpp:738-808 for one domain (layer 0 is the only layer).
-__global__ void k_census(const DomainDesc *Dp, Census *out) {
-    const DomainDesc &D = *Dp;
-    unsigned long long a[5] = {0, 0, 0, 0, 0};
+// Census of src/CAupdate.cpp:738-808 for one domain and its current layer; the smallest
+// CritTimeStep is taken over liquid cells of the layer inside the active window. Each thread reads
+// 16 cells per step with 16-byte loads (the field arrays start on 256-byte boundaries); the tail of
+// fewer than 16 cells is read cell by cell.
+struct CensusCount {
+    unsigned int superheated = 0, undercooled = 0, active = 0, solid = 0, remaining = 0;
     unsigned long long mn = ULLONG_MAX;
-    const long long stride = (long long)gridDim.x * blockDim.x;
-    int cycle = D.cycle;
-    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < D.domain_size; c += stride) {
-        int t = D.ctype[c];
-        int ly = D.layer[c];
-        int cts = D.cts[c];
-        if (ly == 0) {
+    __device__ __forceinline__ void cell(long long c, int t, int ly, int cts, int cycle, int layer, long long w_lo,
+                                         long long w_hi) {
+        if (ly == layer) {
             if (t == kLiquid) {
                 if (cts > cycle)
-                    a[0]++;
+                    superheated++;
                 else
-                    a[1]++;
-                if (c < D.active_size && (unsigned long long)cts < mn)
-                    mn = (unsigned long long)(long long)cts;
+                    undercooled++;
+                const unsigned long long u = (unsigned long long)(long long)cts;
+                if (c >= w_lo && c < w_hi && u < mn)
+                    mn = u;
             }
             else if (t == kActive)
-                a[2]++;
+                active++;
             else if (t == kSolid)
-                a[3]++;
+                solid++;
         }
         else if (t == kLiquid) {
-            a[4]++;
+            remaining++;
         }
     }
+};
+
+__global__ void __launch_bounds__(256) k_census(const DomainDesc *Dp, Census *out) {
+    const DomainDesc &D = *Dp;
+    const int8_t *ctype = D.ctype, *lay = D.layer;
+    const int32_t *ctsp = D.cts;
+    const long long N = D.domain_size;
+    const int cycle = D.cycle, layer = D.layer_no;
+    const long long plane = (long long)D.mx * D.my;
+    const long long w_lo = plane * D.z_lo, w_hi = plane * D.z_end;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long tid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    CensusCount k;
+    const long long n16 = N / 16;
+    for (long long q = tid; q < n16; q += stride) {
+        const int4 t16 = __ldcs(reinterpret_cast<const int4 *>(ctype) + q);
+        const int4 l16 = __ldcs(reinterpret_cast<const int4 *>(lay) + q);
+        int4 c4[4];
+#pragma unroll
+        for (int u = 0; u < 4; u++)
+            c4[u] = __ldcs(reinterpret_cast<const int4 *>(ctsp) + 4 * q + u);
+        const int tw[4] = {t16.x, t16.y, t16.z, t16.w}, lw[4] = {l16.x, l16.y, l16.z, l16.w};
+#pragma unroll
+        for (int u = 0; u < 4; u++) {
+            const int cv[4] = {c4[u].x, c4[u].y, c4[u].z, c4[u].w};
+#pragma unroll
+            for (int b = 0; b < 4; b++) {
+                const int t = (int)(int8_t)(tw[u] >> (8 * b)), ly = (int)(int8_t)(lw[u] >> (8 * b));
+                k.cell(16 * q + 4 * u + b, t, ly, cv[b], cycle, layer, w_lo, w_hi);
+            }
+        }
+    }
+    for (long long c = 16 * n16 + tid; c < N; c += stride)
+        k.cell(c, ctype[c], lay[c], ctsp[c], cycle, layer, w_lo, w_hi);
+    const unsigned int counts[5] = {k.superheated, k.undercooled, k.active, k.solid, k.remaining};
+#pragma unroll
     for (int q = 0; q < 5; q++) {
-        unsigned long long v = a[q];
+        unsigned long long v = counts[q];
         for (int o = 16; o; o >>= 1)
             v += __shfl_down_sync(0xffffffffu, v, o);
         if ((threadIdx.x & 31) == 0 && v)
             atomicAdd((unsigned long long *)out + q, v);
     }
+    unsigned long long mn = k.mn;
     for (int o = 16; o; o >>= 1) {
         unsigned long long v = __shfl_down_sync(0xffffffffu, mn, o);
         mn = v < mn ? v : mn;
@@ -1343,30 +1386,33 @@ __global__ void k_voronoi(DomainDesc *Dp, const int32_t *seeds, int nseeds, floa
         D.gid[c] = best_i + 1;
 }
 
-// Initially active cells: fresh octahedra and the first records (src/CAinitialize.cpp:1929-2044).
+// Active cells of the active window: fresh octahedra and their records. At admission these are
+// the initially active cells (src/CAinitialize.cpp:1929-2044); at the start of a later layer, the
+// active cells of the moved window (LayerSetup, src/CAinitialize.cpp:2840-2982).
 __global__ void k_init_active(PoolState *P, int dom, int list_slot) {
     if (list_slot < 0)
         list_slot = P->pending; // the list the next cycle consumes
     DomainDesc &D = P->desc[dom];
     long long plane = (long long)D.mx * D.my;
     long long lo = plane, hi = plane * (D.nz - 1);
-    long long zmax = plane * ((long long)D.zbound_high + 1);
-    if (hi > zmax)
-        hi = zmax;
+    if (lo < plane * D.z_lo)
+        lo = plane * D.z_lo;
+    if (hi > plane * D.z_end)
+        hi = plane * D.z_end;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long c0 = lo + (long long)blockIdx.x * blockDim.x; c0 < hi; c0 += stride) {
         long long c = c0 + threadIdx.x;
         bool act = c < hi && D.ctype[c] == kActive;
         if (act)
             make_fresh_octahedron(D, (unsigned int)c);
-        bool listed = act && c < D.active_size;
+        bool listed = act;
         unsigned long long pos = block_reserve(P, list_slot, listed ? 1u : 0u);
         if (listed && pos != ULLONG_MAX) {
             ActiveRec r;
             r.cell = (unsigned int)c;
             r.dl = 0.01f;
             r.cdl_min = 0.0f;
-            r.cts = D.cts[c];
+            r.cts = D.cts_run[c];
             P->rec[list_slot][pos] = r;
             P->rdom[list_slot][pos] = (unsigned int)dom;
             P->rstat[list_slot][pos] = kMaskFresh;
@@ -1401,6 +1447,66 @@ __global__ void k_flush_records(PoolState *P) {
         if (D.dl)
             D.dl[r.cell] = r.dl;
     }
+}
+
+// ---------------------------------------------------------------------------------------------
+// Layer change of a multilayer domain (src/runCA.cpp:344-411).
+
+// Undercooling updates of the ending layer, carried into the next: every liquid or active cell of
+// the window whose LayerID <= layer had UndercoolingCurrent += UndercoolingChange once per executed
+// cycle past its CritTimeStep (src/CAupdate.cpp:228-237).
+__global__ void k_layer_base(const DomainDesc *Dp) {
+    const DomainDesc &D = *Dp;
+    const long long plane = (long long)D.mx * D.my;
+    const long long hi = plane * D.z_end;
+    const long long end = executed_upto(D, D.cycle);
+    for (long long c = plane * D.z_lo + (long long)blockIdx.x * blockDim.x + threadIdx.x; c < hi;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int t = D.ctype[c];
+        if ((t != kLiquid && t != kActive) || D.layer[c] > D.layer_no)
+            continue;
+        const long long n = end - executed_upto(D, D.cts[c]);
+        if (n > 0)
+            D.nu_base[c] += (int32_t)n;
+    }
+}
+
+// DomainShiftAndResize's two reductions (src/CAinitialize.cpp:2781-2812): the lowest z of an
+// active cell and the highest z of a cell of the next layer. out = {INT_MAX, INT_MIN} on entry.
+__global__ void k_layer_bounds(const DomainDesc *Dp, int next_layer, int *out) {
+    const DomainDesc &D = *Dp;
+    const long long plane = (long long)D.mx * D.my;
+    int zmin = INT_MAX, zmax = INT_MIN;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < D.domain_size;
+         c += (long long)gridDim.x * blockDim.x) {
+        const int z = (int)(c / plane);
+        if (D.ctype[c] == kActive)
+            zmin = min(zmin, z);
+        if (D.layer[c] == next_layer)
+            zmax = max(zmax, z);
+    }
+    for (int o = 16; o; o >>= 1) {
+        zmin = min(zmin, __shfl_down_sync(0xffffffffu, zmin, o));
+        zmax = max(zmax, __shfl_down_sync(0xffffffffu, zmax, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        if (zmin != INT_MAX)
+            atomicMin(out, zmin);
+        if (zmax != INT_MIN)
+            atomicMax(out + 1, zmax);
+    }
+}
+
+// The CritTimeStep the step uses this layer: the cell's own inside the window for LayerID <= layer,
+// INT_MAX elsewhere (src/CAupdate.cpp:218-231 visits only window cells, and grows those with
+// LayerID <= layernumber).
+__global__ void k_layer_gate(const DomainDesc *Dp) {
+    const DomainDesc &D = *Dp;
+    const long long plane = (long long)D.mx * D.my;
+    const long long lo = plane * D.z_lo, hi = plane * D.z_end;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < D.domain_size;
+         c += (long long)gridDim.x * blockDim.x)
+        D.cts_run[c] = (c >= lo && c < hi && D.layer[c] <= D.layer_no) ? D.cts[c] : INT_MAX;
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -1446,9 +1552,16 @@ void unpin_problem(Problem &p) {
     p.pinned = false;
 }
 
+// Multilayer problems keep the per-cell octahedron state for the whole domain (the active window
+// moves up layer by layer), plus the per-layer CritTimeStep gate and the undercooling carried over.
+static size_t octahedron_cells(const Problem &p) {
+    return p.cfg.number_of_layers > 1 ? (size_t)p.g.domain_size : (size_t)p.g.active_size;
+}
+
 size_t Pool::slot_bytes(const Problem &p) {
-    size_t N = (size_t)p.g.domain_size, A = (size_t)p.g.active_size;
-    return N * (1 + 4 + 4 + 1 + 4) + A * (4 + 12 + 104 + 8 + 4) + p.nuclei_loc.size() * 8 + 64 * 1024;
+    size_t N = (size_t)p.g.domain_size, A = octahedron_cells(p);
+    size_t multilayer = p.cfg.number_of_layers > 1 ? N * 8 : 0;
+    return N * (1 + 4 + 4 + 1 + 4) + A * (4 + 12 + 104 + 8 + 4) + multilayer + p.nuclei_loc.size() * 8 + 64 * 1024;
 }
 
 Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
@@ -1659,7 +1772,12 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     s.used = true;
     s.problem = pp;
     const Geometry &g = p.g;
-    const size_t N = g.domain_size, A = g.active_size, P = p.nuclei_loc.size();
+    const int n_layers = p.cfg.number_of_layers;
+    const bool multilayer = n_layers > 1;
+    if (multilayer && check_mode)
+        throw Unsupported("device-side termination is not offered for multilayer problems (the layer change "
+                          "runs between launches): admit with device_check 0 and run the plain path");
+    const size_t N = g.domain_size, A = octahedron_cells(p), P = p.nuclei_loc.size();
     // every field of the slot in one allocation (256-byte aligned sub-arrays)
     size_t off = 0;
     auto carve = [&](size_t bytes) {
@@ -1669,7 +1787,8 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     };
     const size_t o_ct = carve(N), o_gid = carve(N * 4), o_cts = carve(N * 4), o_ly = carve(N), o_du = carve(N * 4),
                  o_dl = carve(A * 4), o_doc = carve(A * 12), o_cdl = carve(A * 104), o_claim = carve(A * 8),
-                 o_pos = carve(A * 4), o_nl = carve(P * 4), o_nt = carve(P * 4);
+                 o_pos = carve(A * 4), o_nl = carve(P * 4), o_nt = carve(P * 4),
+                 o_run = multilayer ? carve(N * 4) : 0, o_base = multilayer ? carve(N * 4) : 0;
     char *slab = nullptr;
     CUDA_OK(cudaMalloc(&slab, off));
     s.allocs.push_back(slab);
@@ -1686,6 +1805,8 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     d.cdl = (float *)(slab + o_cdl);
     d.claim = (unsigned long long *)(slab + o_claim);
     d.pos = (unsigned int *)(slab + o_pos);
+    d.cts_run = multilayer ? (int32_t *)(slab + o_run) : d.cts;
+    d.nu_base = multilayer ? (int32_t *)(slab + o_base) : nullptr;
     int32_t *dnl = (int32_t *)(slab + o_nl);
     int32_t *dnt = (int32_t *)(slab + o_nt);
     // nuclei in time order; ties keep the reference's order (order does not change results)
@@ -1707,6 +1828,8 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     CUDA_OK(cudaMemsetAsync(d.dl, 0, A * 4, st));
     CUDA_OK(cudaMemsetAsync(d.claim, 0xff, A * 8, st));
     CUDA_OK(cudaMemsetAsync(d.pos, 0xff, A * 4, st)); // kNoRecord
+    if (multilayer)
+        CUDA_OK(cudaMemsetAsync(d.nu_base, 0, N * 4, st));
     if (P) {
         CUDA_OK(cudaMemcpyAsync(dnl, nl.data(), P * 4, cudaMemcpyHostToDevice, st));
         CUDA_OK(cudaMemcpyAsync(dnt, nt.data(), P * 4, cudaMemcpyHostToDevice, st));
@@ -1724,9 +1847,13 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     d.xoff = g.xoff;
     d.yoff = g.yoff;
     d.zbound_high = g.zbound_high;
+    d.layer_no = 0;
+    d.n_layers = n_layers;
+    d.z_lo = g.zbound_low;
+    d.z_end = g.zbound_low + g.nz_active;
     d.check_mode = check_mode;
     d.domain_size = g.domain_size;
-    d.active_size = g.active_size;
+    d.active_size = (long long)A;
     d.du_value = p.du_value;
     long long liquid = 0;
     int zero_du = 0;
@@ -1741,6 +1868,13 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     d.zero_du = zero_du;
     host_desc_[slot] = d;
     push_desc(slot);
+    if (multilayer) {
+        k_layer_gate<<<num_sms_ * 4, 256, 0, st>>>(ddesc_ + slot);
+        CUDA_OK(cudaGetLastError());
+        static const int one = 1;
+        CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, multilayer), &one, sizeof(int),
+                                cudaMemcpyHostToDevice, st));
+    }
     ensure_growth(slot, 4096);
     if (!p.voronoi_seeds.empty() || p.cfg.simulation_type == "S") {
         int nseeds = (int)(p.voronoi_seeds.size() / 3);
@@ -2114,6 +2248,69 @@ void Pool::set_cycle(int slot, int cycle) {
     push_desc(slot);
 }
 
+void Pool::next_layer(int slot, std::string &log) {
+    // src/runCA.cpp:344-405: DomainShiftAndResize, then LayerSetup on the moved window
+    CUDA_OK(cudaSetDevice(device_));
+    cudaStream_t st = S(stream_);
+    sync_state();
+    DomainDesc d = host_desc_.at(slot);
+    if (d.layer_no + 1 >= d.n_layers || !d.nu_base)
+        throw std::logic_error("next_layer: the slot has no further layer");
+    const unsigned blocks = (unsigned)num_sms_ * 4;
+    k_layer_base<<<blocks, 256, 0, st>>>(ddesc_ + slot);
+    CUDA_OK(cudaGetLastError());
+    int bounds[2] = {INT_MAX, INT_MIN};
+    int *dbounds = nullptr;
+    CUDA_OK(cudaMalloc(&dbounds, sizeof(bounds)));
+    CUDA_OK(cudaMemcpyAsync(dbounds, bounds, sizeof(bounds), cudaMemcpyHostToDevice, st));
+    k_layer_bounds<<<blocks, 256, 0, st>>>(ddesc_ + slot, d.layer_no + 1, dbounds);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaMemcpyAsync(bounds, dbounds, sizeof(bounds), cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    CUDA_OK(cudaFree(dbounds));
+    // the new bottom is one plane below the lowest active cell, the new top the highest cell of the
+    // next layer (src/CAinitialize.cpp:2776-2820)
+    if (bounds[0] == INT_MAX || bounds[1] == INT_MIN || bounds[0] - 1 > bounds[1] || bounds[1] >= d.nz)
+        throw DeviceError("layer change: no active cell or no cell of the next layer");
+    const int z_lo = bounds[0] - 1, z_hi = bounds[1];
+    std::ostringstream s;
+    s << "New domain bottom at Z = " << z_lo << ", a shift of " << z_lo - d.z_lo << " cells\n";
+    s << "New domain top at Z = " << z_hi << "\n";
+    s << "New active domain height is " << z_hi - z_lo + 1 << "\n";
+    s << "Resize executed\n";
+    d.layer_no += 1;
+    d.z_lo = z_lo;
+    d.z_end = z_hi + 1;
+    d.nz_active = z_hi - z_lo + 1;
+    d.zbound_high = z_hi;
+    d.cycle = 0;
+    d.nuc_cursor = 0;
+    d.nn = 0;
+    d.n_jumps = 0;
+    host_desc_[slot] = d;
+    push_desc(slot);
+    k_layer_gate<<<blocks, 256, 0, st>>>(ddesc_ + slot);
+    CUDA_OK(cudaGetLastError());
+    // LayerSetup: the records of the ended layer leave the list (re-labelled to the pool's finished
+    // placeholder domain, dropped by the next growth pass); the window's octahedron arrays start from
+    // zero (src/CAinitialize.cpp:2850-2852); every active cell of the new window gets a fresh
+    // octahedron and a record
+    k_drop_domain<<<num_sms_ * 2, 256, 0, st>>>(dstate_, (unsigned)slot, (unsigned)max_domains_);
+    CUDA_OK(cudaGetLastError());
+    CUDA_OK(cudaMemsetAsync(d.pos, 0xff, (size_t)d.active_size * 4, st));
+    {
+        const size_t plane = (size_t)d.mx * d.my, o = plane * d.z_lo, n = plane * (d.z_end - d.z_lo);
+        CUDA_OK(cudaMemsetAsync(d.dl + o, 0, n * 4, st));
+        CUDA_OK(cudaMemsetAsync(d.doc + 3 * o, 0, n * 12, st));
+        CUDA_OK(cudaMemsetAsync(d.cdl + 26 * o, 0, n * 104, st));
+    }
+    k_init_active<<<num_sms_ * 4, 256, 0, st>>>(dstate_, slot, -1);
+    CUDA_OK(cudaGetLastError());
+    s << "New layer setup, GN dimensions are " << d.mx << " " << 0 << " " << d.nz_active << "\n";
+    s << "New layer ghost nodes initialized\n";
+    log += s.str();
+}
+
 void Pool::copy_out_raw(int slot, int32_t *grain_id, int8_t *cell_type) {
     CUDA_OK(cudaSetDevice(device_));
     const DomainDesc &d = host_desc_.at(slot);
@@ -2136,14 +2333,15 @@ void Pool::flush_records() {
 void Pool::copy_octahedra(int slot, float *dl, float *doc, float *cdl) {
     flush_records();
     const DomainDesc &d = host_desc_.at(slot);
-    size_t A = slots_.at(slot).problem->g.active_size;
+    // the current layer's window (the whole allocation's prefix for single-layer problems)
+    const size_t plane = (size_t)d.mx * d.my, o = plane * d.z_lo, A = plane * (d.z_end - d.z_lo);
     cudaStream_t st = S(stream_);
     if (dl)
-        CUDA_OK(cudaMemcpyAsync(dl, d.dl, A * 4, cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(dl, d.dl + o, A * 4, cudaMemcpyDeviceToHost, st));
     if (doc)
-        CUDA_OK(cudaMemcpyAsync(doc, d.doc, A * 12, cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(doc, d.doc + 3 * o, A * 12, cudaMemcpyDeviceToHost, st));
     if (cdl)
-        CUDA_OK(cudaMemcpyAsync(cdl, d.cdl, A * 104, cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaMemcpyAsync(cdl, d.cdl + 26 * o, A * 104, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
 }
 
@@ -2159,10 +2357,11 @@ void Pool::copy_out(int slot, int32_t *grain_id, int32_t *cell_type) {
 }
 
 int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_s) {
-    // src/runCA.cpp:283-342 for one layer
+    // src/runCA.cpp:282-411: the layer loop, each layer's cycles until no liquid of the layer is left
     const Problem &p = *slots_.at(slot).problem;
     bool jump_type = p.cfg.simulation_type == "S" || p.cfg.simulation_type == "R";
     auto t0 = std::chrono::steady_clock::now();
+    auto t_layer = t0;
     cudaEvent_t ev0, ev1;
     CUDA_OK(cudaEventCreate(&ev0));
     CUDA_OK(cudaEventCreate(&ev1));
@@ -2187,8 +2386,19 @@ int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_
           << " Undercooled liquid cells = " << c.undercooled << " Number of nucleation events this layer " << d.nn
           << " Remaining liquid cells in future layers of this simulation = " << c.remaining << "\n";
         log += s.str();
-        if (c.superheated + c.undercooled == 0)
-            break;
+        if (c.superheated + c.undercooled == 0) {
+            if (d.layer_no + 1 >= d.n_layers)
+                break;
+            const int layer = d.layer_no;
+            next_layer(slot, log);
+            double secs = std::chrono::duration<double>(std::chrono::steady_clock::now() - t_layer).count();
+            t_layer = std::chrono::steady_clock::now();
+            std::ostringstream s2;
+            s2 << "Time for layer number " << layer << " was " << secs << " s, starting layer " << layer + 1 << "\n";
+            log += s2.str();
+            cycle = 0;
+            continue;
+        }
         if (jump_type && c.undercooled == 0) {
             unsigned long long next = c.next_cts;
             if ((next - (unsigned long long)(long long)cycle) > 5000) {

@@ -454,8 +454,8 @@ void initialize_problem(Problem &p, std::string &log) {
         throw Unsupported("Problem type R (temperature data from files) is not supported by the B200 solver");
     if (c.simulation_type != "C" && c.simulation_type != "S")
         throw std::runtime_error("Unknown problem type \"" + c.simulation_type + "\"");
-    if (c.number_of_layers != 1)
-        throw Unsupported("The B200 solver supports single-layer problems only (Number of layers: 1)");
+    if (c.number_of_layers < 1 || c.number_of_layers > 127)
+        throw Unsupported("Number of layers must be between 1 and 127 (LayerID is stored in 8 bits)");
     if (c.simulation_type == "S" && c.use_substrate_file)
         throw Unsupported("Substrate files are not supported by the B200 solver");
 

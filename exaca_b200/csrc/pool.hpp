@@ -96,6 +96,16 @@ struct DomainDesc {
     long long liquid_shard[kLiquidShards]; // minus the captures, spread over shards to avoid contention
     int jump_lo[kMaxJumps];
     int jump_hi[kMaxJumps];
+    // Multilayer problems (src/runCA.cpp:282-411). cts_run is the CritTimeStep the step uses: the
+    // cell's own for cells of the active window [z_lo, z_end) whose LayerID <= layer_no, INT_MAX
+    // for every other cell (the reference's step does not touch them this layer). nu_base holds per
+    // cell the undercooling updates of earlier layers (UndercoolingCurrent is never reset). For
+    // single-layer problems cts_run == cts and nu_base is null.
+    int32_t *cts_run;
+    int32_t *nu_base;
+    int layer_no;
+    int n_layers;
+    int z_lo, z_end;
 };
 
 // Pool-level device state.
@@ -125,7 +135,7 @@ struct PoolState {
     int compact;              // 1: this cycle's growth pass writes the survivors to list cur ^ 1
     int error;
     int n_domains;
-    int pad;
+    int multilayer; // 1 once a multilayer domain was admitted (its records carry earlier layers' updates)
     DomainDesc *desc;
     unsigned long long stat[kStatShards][kNumStats];
     unsigned int blocks_done;      // last-block detection of the separate capture kernel
@@ -203,8 +213,12 @@ class Pool {
     // writes the diagonal lengths held in the active records back to the per-cell array
     void flush_records();
     // Reference-equivalent run of one slot to completion with the reference's 1000-cycle census,
-    // stdout progress lines and type-S cycle jumps (src/runCA.cpp:290-342).
+    // stdout progress lines, type-S cycle jumps and, for multilayer problems, the move of the active
+    // window between layers (src/runCA.cpp:282-411).
     int run_plain(int slot, std::string &log, double *nucl_s, double *capture_s);
+    // Ends the current layer of a multilayer slot and sets up the next one: DomainShiftAndResize
+    // and LayerSetup (src/CAinitialize.cpp:2772-2982). Appends the reference's lines to `log`.
+    void next_layer(int slot, std::string &log);
     // device time (CUDA events on the pool stream) of the last run_plain
     double last_run_ms() const { return last_run_ms_; }
     // runs n cycles as separate per-pass kernels with CUDA events around each launch

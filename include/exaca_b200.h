@@ -60,7 +60,11 @@ typedef struct {
     int done;           /* 1 once the domain met the reference's termination test */
     int nn;             /* nucleation events so far */
     int error;          /* device error flags (0 = none) */
-    int64_t liquid;     /* liquid cells left */
+    int64_t liquid;     /* liquid cells left (device-checked single-layer slots) */
+    int layer;          /* current layer (layernumber, src/runCA.cpp:282) */
+    int window_z_lo;    /* the layer's active window: z planes [window_z_lo, window_z_lo + window_nz) */
+    int window_nz;      /* (ZBound_Low and nzActive, src/runCA.cpp:96-102) */
+    int reserved;
 } exaca_domain_status;
 
 /* Work counters of a pool since its creation (summed over all domains). */
@@ -160,7 +164,9 @@ double exaca_pool_last_run_ms(exaca_pool *pool);
 int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms);
 /* Device->host copy of GrainID and CellType (src/runCA.cpp:423-424); NULL skips a field. */
 int exaca_pool_copy_out(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *cell_type);
-/* Active-window octahedron state (DiagonalLength, DOCenter x3, CritDiagonalLength x26). */
+/* Active-window octahedron state (DiagonalLength, DOCenter x3, CritDiagonalLength x26) of the
+ * slot's current layer: window_nz * mx * my cells from plane window_z_lo (exaca_pool_status), the
+ * reference's window arrays (src/runCA.cpp:147-151, resized per layer at :352-356). */
 int exaca_pool_copy_octahedra(exaca_pool *pool, int slot, float *dl, float *doc, float *cdl);
 /* Frees a slot's device memory. */
 int exaca_pool_retire(exaca_pool *pool, int slot);

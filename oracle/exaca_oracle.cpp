@@ -15,12 +15,15 @@
 //   void *oracle_create(const char *input_file, const char *data_dir)   NULL on error
 //   const char *oracle_error(void)
 //   int  oracle_geometry(void *o, long long *out6)    mx, my, nz, nz_active, domain size, active size
-//   int  oracle_step(void *o, int n_cycles)            n raw cycles (no 1000-cycle check)
-//   int  oracle_run(void *o, int *final_cycle)          to termination, as RunProgram_Reduced does
+//                                                      (of the current layer's window)
+//   int  oracle_step(void *o, int n_cycles)            n raw cycles of the current layer (no check)
+//   int  oracle_run(void *o, int *final_cycle)          to termination of the last layer, as
+//                                                      RunProgram_Reduced does
 //   int  oracle_cycle(void *o)
 //   int  oracle_fields(void *o, int *cell_type, int *grain_id, float *dl, float *doc, float *cdl)
 //   void oracle_free(void *o)
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -133,8 +136,6 @@ Input read_input(const std::string &path, const std::string &data_dir) {
         I.nz = I.spot_radius + 3 + (I.layers - 1) * I.layer_height;
         I.nx = 4 + 2 * I.spot_radius + I.spot_offset * (I.nspx - 1);
         I.ny = 4 + 2 * I.spot_radius + I.spot_offset * (I.nspy - 1);
-        if (I.layers != 1)
-            throw std::runtime_error("oracle: single-layer problems only");
     }
     else {
         throw std::runtime_error("oracle: problem types C and S only");
@@ -154,7 +155,7 @@ struct Oracle {
     std::vector<float> GrainUnitVector;
     std::vector<int> NucleiLocation, NucleationTimes;
     double A, B, C, D;
-    int cycle = 0, nn = 0;
+    int cycle = 0, nn = 0, layer = 0;
     std::vector<int> SteeringVector;
 
     long idx(int k, int i, int j) const { return (long)k * MX * MY + (long)i * MY + j; }
@@ -301,27 +302,29 @@ void initialise(Oracle &o) {
         int nspots = I.nspx * I.nspy;
         float iso = (I.R / I.G) * I.deltat / I.deltax;
         int between = I.spot_radius / iso + (I.freezing / I.R) / I.deltat;
-        for (int n = 0; n < nspots; n++) {
-            int xs = 2 + I.spot_radius + (n % I.nspx) * I.spot_offset;
-            int ys = 2 + I.spot_radius + (n / I.nspx) * I.spot_offset;
-            int zs = I.spot_radius + 2;
-            for (int k = 0; k < o.nzActive; k++) {
-                float dz = (float)(zs - k);
-                for (int i = 0; i < MX; i++) {
-                    float dx = (float)(xs - (i + o.XOff));
-                    for (int j = 0; j < MY; j++) {
-                        float dy = (float)(ys - (j + o.YOff));
-                        float d = sqrtf(dx * dx + dy * dy + dz * dz);
-                        if (d <= I.spot_radius) {
-                            long p = o.idx(k, i, j);
-                            o.CritTimeStep[p] = 1 + (int)(((float)(I.spot_radius) - d) / iso) + between * n;
-                            o.UndercoolingChange[p] = I.R * I.deltat;
-                            o.LayerID[p] = 0;
+        // every layer's spots, later layers overwriting earlier ones
+        for (int layer = 0; layer < I.layers; layer++)
+            for (int n = 0; n < nspots; n++) {
+                int xs = 2 + I.spot_radius + (n % I.nspx) * I.spot_offset;
+                int ys = 2 + I.spot_radius + (n / I.nspx) * I.spot_offset;
+                int zs = I.spot_radius + 2 + I.layer_height * layer;
+                for (int k = 0; k < o.nzActive; k++) {
+                    float dz = (float)(zs - (k + I.layer_height * layer));
+                    for (int i = 0; i < MX; i++) {
+                        float dx = (float)(xs - (i + o.XOff));
+                        for (int j = 0; j < MY; j++) {
+                            float dy = (float)(ys - (j + o.YOff));
+                            float d = sqrtf(dx * dx + dy * dy + dz * dz);
+                            if (d <= I.spot_radius) {
+                                long p = o.idx(k + layer * I.layer_height, i, j);
+                                o.CritTimeStep[p] = 1 + (int)(((float)(I.spot_radius) - d) / iso) + between * n;
+                                o.UndercoolingChange[p] = I.R * I.deltat;
+                                o.LayerID[p] = layer;
+                            }
                         }
                     }
                 }
             }
-        }
     }
     o.NA = (long)MX * MY * o.nzActive;
     o.DiagonalLength.assign(o.NA, 0.0f);
@@ -503,7 +506,7 @@ void nucleation(Oracle &o) {
     const int MX = o.MX, MY = o.MY;
     for (size_t n = 0; n < o.NucleiLocation.size(); n++) {
         long g = o.NucleiLocation[n];
-        if (o.cycle >= o.NucleationTimes[n] && o.CellType[g] == Liquid && o.LayerID[g] <= 0) {
+        if (o.cycle >= o.NucleationTimes[n] && o.CellType[g] == Liquid && o.LayerID[g] <= o.layer) {
             o.CellType[g] = TemporaryUpdate;
             int GlobalZ = g / (MX * MY);
             int Rem = g % (MX * MY);
@@ -603,7 +606,7 @@ void cell_capture(Oracle &o) {
         int Rem = D3D1 % (MX * MY);
         long Global = (long)(RankZ + o.ZBound_Low) * MX * MY + Rem;
         int ct = o.CellType[Global];
-        if (o.LayerID[Global] <= 0 && ct != Solid && o.cycle > o.CritTimeStep[Global]) {
+        if (o.LayerID[Global] <= o.layer && ct != Solid && o.cycle > o.CritTimeStep[Global]) {
             o.UndercoolingCurrent[Global] += o.UndercoolingChange[Global] * ((ct == Liquid) + (ct == Active));
             if (ct == Active)
                 o.SteeringVector[numSteer++] = (int)D3D1;
@@ -647,7 +650,7 @@ void cell_capture(Oracle &o) {
 int check(Oracle &o) {
     unsigned long sh = 0, uc = 0;
     for (long p = 0; p < o.N; p++)
-        if (o.LayerID[p] == 0 && o.CellType[p] == Liquid) {
+        if (o.LayerID[p] == o.layer && o.CellType[p] == Liquid) {
             if (o.CritTimeStep[p] > o.cycle)
                 sh++;
             else
@@ -660,13 +663,49 @@ int check(Oracle &o) {
         for (long D3D1 = 0; D3D1 < o.NA; D3D1++) {
             long g = D3D1 + (long)o.ZBound_Low * o.MX * o.MY;
             unsigned long cts = (unsigned long)(o.CritTimeStep[g]);
-            if (o.CellType[g] == Liquid && o.LayerID[g] == 0 && cts < next)
+            if (o.CellType[g] == Liquid && o.LayerID[g] == o.layer && cts < next)
                 next = cts;
         }
         if ((next - o.cycle) > 5000)
             o.cycle = next - 1;
     }
     return 0;
+}
+
+// src/CAinitialize.cpp:2772-2837 (one rank): the window's new bottom is one plane below the lowest
+// active cell, its new top the highest cell of the next layer
+void domain_shift_and_resize(Oracle &o) {
+    int lo = INT_MAX, hi = INT_MIN;
+    const long plane = (long)o.MX * o.MY;
+    for (long p = 0; p < o.N; p++) {
+        int z = (int)(p / plane);
+        if (o.CellType[p] == Active && z < lo)
+            lo = z;
+        if (o.LayerID[p] == o.layer + 1 && z > hi)
+            hi = z;
+    }
+    o.ZBound_Low = lo - 1;
+    o.ZBound_High = hi;
+    o.nzActive = o.ZBound_High - o.ZBound_Low + 1;
+    o.NA = plane * o.nzActive;
+}
+
+// src/CAinitialize.cpp:2840-2982: window arrays zeroed, fresh octahedra for the window's active cells
+void layer_setup(Oracle &o) {
+    const int MX = o.MX, MY = o.MY;
+    o.DiagonalLength.assign(o.NA, 0.0f);
+    o.DOCenter.assign(3 * o.NA, 0.0f);
+    o.CritDiagonalLength.assign(26 * o.NA, 0.0f);
+    o.SteeringVector.assign(o.NA, 0);
+    for (long D3D1 = 0; D3D1 < o.NA; D3D1++) {
+        int RankZ = D3D1 / (MX * MY);
+        int Rem = D3D1 % (MX * MY);
+        int RankX = Rem / MY, RankY = Rem % MY;
+        int GlobalZ = RankZ + o.ZBound_Low;
+        long g = (long)GlobalZ * MX * MY + Rem;
+        if (o.CellType[g] == Active)
+            fresh_octahedron(o, D3D1, RankX + o.XOff, RankY + o.YOff, GlobalZ, o.GrainID[g]);
+    }
 }
 
 } // namespace
@@ -712,17 +751,26 @@ int oracle_step(void *p, int n) {
     return 0;
 }
 
-// src/runCA.cpp:290-342 for one layer
+// src/runCA.cpp:282-411: every layer's cycles, the window moved between layers
 int oracle_run(void *p, int *final_cycle) {
     Oracle &o = *static_cast<Oracle *>(p);
-    int XSwitch = 0;
-    do {
-        o.cycle++;
-        nucleation(o);
-        cell_capture(o);
-        if (o.cycle % 1000 == 0)
-            XSwitch = check(o);
-    } while (XSwitch == 0);
+    for (; o.layer < o.in.layers; o.layer++) {
+        int XSwitch = 0;
+        o.nn = 0;
+        do {
+            o.cycle++;
+            nucleation(o);
+            cell_capture(o);
+            if (o.cycle % 1000 == 0)
+                XSwitch = check(o);
+        } while (XSwitch == 0);
+        if (o.layer != o.in.layers - 1) {
+            domain_shift_and_resize(o);
+            layer_setup(o);
+            o.cycle = 0;
+        }
+    }
+    o.layer = o.in.layers - 1;
     *final_cycle = o.cycle;
     return 0;
 }

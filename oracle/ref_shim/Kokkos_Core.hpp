@@ -55,7 +55,10 @@ template <class T> struct rank_of<T *> {
 };
 // With EXACA_SHIM_DUMP_DIR set, the storage of the views named below is written to
 // $EXACA_SHIM_DUMP_DIR/<label>.bin when it is released, i.e. the reference's final state at the
-// end of RunProgram_Reduced. Used to build golden arrays; the reference code is not touched.
+// end of RunProgram_Reduced. A label's earlier dump is kept as <label>.prev.bin: in multilayer runs
+// the resized device views (released first) hold the final state and the host mirrors, released
+// last, still hold the first layer's storage. Used to build golden arrays; the reference code is
+// not touched.
 inline bool dump_label(const std::string &l) {
     static const char *names[] = {"GrainID", "CellType", "DiagonalLength", "DOCenter", "CritDiagonalLength",
                                   "UndercoolingCurrent", "CritTimeStep", "UndercoolingChange", "LayerID"};
@@ -72,6 +75,7 @@ struct Storage {
         const char *dir = std::getenv("EXACA_SHIM_DUMP_DIR");
         if (dir && ptr && dump_label(label)) {
             std::string f = std::string(dir) + "/" + label + ".bin";
+            std::rename(f.c_str(), (std::string(dir) + "/" + label + ".prev.bin").c_str());
             if (FILE *fp = std::fopen(f.c_str(), "wb")) {
                 std::fwrite(ptr, 1, bytes, fp);
                 std::fclose(fp);

@@ -47,8 +47,8 @@ Number of spots in x: {sx}
 Number of spots in y: {sy}
 Offset between spot centers (in microns): {off}
 Radii of spots (in microns): {rad}
-Number of layers: 1
-Offset between layers (in cells): 10
+Number of layers: {layers}
+Offset between layers (in cells): {lh}
 "N", where the time step = deltax/(Steady State Velocity * N): {N}
 Substrate grain spacing (in microns): {spacing}
 ***Output data printing options: (Y or N) which data should be printed***
@@ -72,16 +72,22 @@ def random_c(seed, outdir):
     return path
 
 
-def random_s(seed, outdir):
+def random_s(seed, outdir, multilayer=False):
+    """Seeded random spot-melt input; with multilayer, 2-4 layers 3 to R cells apart (drawn after
+    the single-layer parameters, so those stay the same for a seed)."""
     r = np.random.default_rng(seed)
     name = f"rs{seed}"
     rad = int(r.integers(6, 13))
-    txt = S_TEMPLATE.format(
+    prm = dict(
         name=name, out=outdir, sx=int(r.integers(1, 3)), sy=int(r.integers(1, 3)), rad=rad,
         off=int(r.integers(rad // 2, rad + 4)), G=float(10 ** r.uniform(5, 6.5)), R=float(10 ** r.uniform(5, 6.5)),
         density=round(float(10 ** r.uniform(0, 3)), 3), dtn=round(float(r.uniform(1, 6)), 2),
         sigma=round(float(r.uniform(0.2, 1.0)), 2), N=int(r.integers(10, 31)),
-        spacing=round(float(r.uniform(4, 12)), 2))
+        spacing=round(float(r.uniform(4, 12)), 2), layers=1, lh=10)
+    if multilayer:
+        prm["layers"] = int(r.integers(2, 5))
+        prm["lh"] = int(r.integers(3, rad + 1))
+    txt = S_TEMPLATE.format(**prm)
     path = os.path.join(outdir, name + ".txt")
     open(path, "w").write(txt)
     return path

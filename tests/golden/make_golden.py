@@ -10,7 +10,8 @@ tests/golden/inputs/, and stores per case in tests/golden/<case>.npz:
   final_*      GrainID and CellType (full rank-local arrays) at the end of the run,
                captured by the shim when the reference releases its views
   sha_*        SHA-256 of the reference's .vtk and _Misorientations.vtk output files, of the final
-               DiagonalLength array, and of DOCenter / CritDiagonalLength over cells with DL != 0
+               DiagonalLength array (for multilayer runs: of the last layer's active window), and of
+               DOCenter / CritDiagonalLength over cells with DL != 0
   cycle        the final cycle written to the .log
   census       the reference's every-1000-cycle stdout lines
 
@@ -86,9 +87,16 @@ def run_case(case):
         cycle = int(re.search(r"output written at cycle (\d+)", log).group(1))
         gid = np.fromfile(os.path.join(dump, "GrainID.bin"), np.int32)
         ct = np.fromfile(os.path.join(dump, "CellType.bin"), np.int32)
-        dl = np.fromfile(os.path.join(dump, "DiagonalLength.bin"), np.float32)
-        doc = np.fromfile(os.path.join(dump, "DOCenter.bin"), np.float32).reshape(-1, 3)
-        cdl = np.fromfile(os.path.join(dump, "CritDiagonalLength.bin"), np.float32).reshape(-1, 26)
+        # multilayer: the octahedron views were resized, and their final storage is the dump before
+        # the host mirror's (which still holds the first layer's window)
+        layers = 1
+        for ln in open(src):
+            if ln.startswith("Number of layers"):
+                layers = int(ln.split(":", 1)[1])
+        octa = ".prev.bin" if layers > 1 else ".bin"
+        dl = np.fromfile(os.path.join(dump, "DiagonalLength" + octa), np.float32)
+        doc = np.fromfile(os.path.join(dump, "DOCenter" + octa), np.float32).reshape(-1, 3)
+        cdl = np.fromfile(os.path.join(dump, "CritDiagonalLength" + octa), np.float32).reshape(-1, 26)
         ever = dl != 0
         out = dict(
             init_cell_type=dbg["CellType"].astype(np.int8),

@@ -52,6 +52,10 @@ class Oracle:
         return lib().oracle_cycle(self.h)
 
     def fields(self):
+        """Cell fields, and the octahedron arrays of the current layer's active window."""
+        g = (ctypes.c_longlong * 6)()
+        lib().oracle_geometry(self.h, g)
+        self.nz_active, self.na = int(g[3]), int(g[5])
         ct = np.empty(self.n, np.int32)
         gid = np.empty(self.n, np.int32)
         dl = np.empty(self.na, np.float32)

@@ -95,13 +95,17 @@ def test_malformed_inputs(lib, tmp_path, lines, code, msg):
         assert msg in str(e.value)
 
 
-def test_unsupported_multilayer(lib, tmp_path):
+def test_multilayer_problem_and_layer_limit(lib, tmp_path):
     lines = open(input_path("SmallSpotMelt")).read().splitlines()
-    lines = [("Number of layers: 2" if l.startswith("Number of layers") else l) for l in lines]
+    two = [("Number of layers: 2" if l.startswith("Number of layers") else l) for l in lines]
+    p = ex.Problem.from_file(write(tmp_path, "ml.txt", two))
+    assert p.geometry.nz > p.geometry.nz_active
+    # LayerID is kept in 8 bits on the device
+    many = [("Number of layers: 200" if l.startswith("Number of layers") else l) for l in lines]
     with pytest.raises(ex.ExacaError) as e:
-        ex.Problem.from_file(write(tmp_path, "ml.txt", lines))
+        ex.Problem.from_file(write(tmp_path, "ml200.txt", many))
     assert e.value.code == -2
-    assert "single-layer" in str(e.value)
+    assert "between 1 and 127" in str(e.value)
 
 
 def test_missing_input_file(lib):

@@ -1,6 +1,7 @@
 """GPU solver vs the CPU restatement oracle on seeded random problems of both kinds: identical
 CellType, GrainID and DiagonalLength after the same raw cycle counts, and identical final state and
-cycle at termination (bit-exact; the arithmetic is integer and reference-order floating point)."""
+cycle at termination (bit-exact; the arithmetic is integer and reference-order floating point),
+single-layer and multilayer (the active window moved between layers)."""
 import numpy as np
 import pytest
 
@@ -60,4 +61,31 @@ def test_spot_melt_random_to_termination(lib, tmp_path, seed):
     compare(pool, slot, o, "after init")
     assert pool.run_plain(slot) == o.run()
     compare(pool, slot, o, "final")
+    pool.close()
+
+
+@pytest.mark.parametrize("seed", range(4))
+def test_spot_melt_multilayer_random_to_termination(lib, tmp_path, seed):
+    inp = random_s(4000 + seed, str(tmp_path), multilayer=True)
+    p = ex.Problem.from_file(inp)
+    o = Oracle(inp)
+    pool = ex.Pool(0, list_capacity=p.geometry.domain_size)
+    slot = pool.admit(p, device_check=False)
+    compare(pool, slot, o, "after init")
+    assert pool.run_plain(slot) == o.run()
+    st = pool.status(slot)
+    assert st.layer == int(open(inp).read().split("Number of layers:")[1].split()[0]) - 1
+    o.fields()  # refreshes the oracle's window geometry
+    assert (st.window_nz, st.window_nz * p.geometry.mx * p.geometry.my) == (o.nz_active, o.na)
+    compare(pool, slot, o, "final")
+    pool.close()
+
+
+def test_multilayer_needs_plain_path(lib, tmp_path):
+    # the layer change runs between launches, so device-side termination is refused
+    p = ex.Problem.from_file(random_s(4100, str(tmp_path), multilayer=True))
+    pool = ex.Pool(0, list_capacity=p.geometry.domain_size)
+    with pytest.raises(ex.ExacaError) as e:
+        pool.admit(p, device_check=True)
+    assert e.value.code == -2
     pool.close()
