@@ -592,16 +592,21 @@ __device__ __forceinline__ float effective_min(const ActiveRec &r, unsigned int 
 }
 
 __device__ __forceinline__ void load_growth(const DomainDesc &D, const ActiveRec &r, double &inc, bool &ok,
-                                            bool multilayer) {
+                                            bool extras) {
     // undercooling after the executed updates since the liquidus (src/CAupdate.cpp:236-237), plus
-    // those of earlier layers
+    // those of earlier layers; the growth table of the cell's UndercoolingChange value
     long long nu = executed_upto(D, D.cycle) - executed_upto(D, r.cts);
-    if (multilayer && D.nu_base)
-        nu += __ldg(D.nu_base + r.cell);
+    const double *table = D.growth;
+    if (extras) {
+        if (D.nu_base)
+            nu += __ldg(D.nu_base + r.cell);
+        if (D.du_class)
+            table += (size_t)__ldg(D.du_class + r.cell) * (size_t)D.growth_len;
+    }
     if (D.zero_du && D.du[r.cell] == 0.0f)
         nu = 0;
     ok = nu >= 0 && nu < D.growth_len;
-    inc = (ok && D.cycle > r.cts) ? __ldg(D.growth + nu) : 0.0;
+    inc = (ok && D.cycle > r.cts) ? __ldg(table + nu) : 0.0;
 }
 
 // Records the growth pass hands to the claim pass go to a global queue together with the state the
@@ -742,7 +747,7 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
                                          unsigned long long n, CycleStats &st) {
     const unsigned int lane = threadIdx.x & 31;
     DomainDesc *desc = P->desc;
-    const bool multilayer = P->multilayer;
+    const bool extras = P->extras;
     const ActiveRec *in = P->rec[cur];
     const unsigned int *in_dom = P->rdom[cur];
     const unsigned int *in_stat = P->rstat[cur];
@@ -769,7 +774,7 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
             if (r.cell != kTombstone) {
                 double inc;
                 bool ok;
-                load_growth(desc[dom], r, inc, ok, multilayer);
+                load_growth(desc[dom], r, inc, ok, extras);
                 keep = grow_record(desc[dom], r, m, inc, ok, effective_min(r, m, mn2), st) != 0;
                 if (!keep)
                     st.dropped++;
@@ -809,7 +814,7 @@ template <int kBatch> __device__ void grow_pass(PoolState *P, CycleStats &st) {
     unsigned int *in_stat = P->rstat[cur];
     const unsigned long long *in_min2 = P->rmin2[cur];
     DomainDesc *desc = P->desc;
-    const bool multilayer = P->multilayer;
+    const bool extras = P->extras;
     unsigned long long tombs = 0;
     const unsigned long long groups = (n + 31) / 32;
     // records are updated in place; dropped ones become tombstones
@@ -845,7 +850,7 @@ template <int kBatch> __device__ void grow_pass(PoolState *P, CycleStats &st) {
                     m[q] &= ~kMaskKeep;
                     in_stat[idx[q]] = m[q];
                 }
-                load_growth(desc[dom[q]], r[q], inc[q], ok[q], multilayer);
+                load_growth(desc[dom[q]], r[q], inc[q], ok[q], extras);
             }
         }
         unsigned int flagged = 0;
@@ -1561,7 +1566,9 @@ static size_t octahedron_cells(const Problem &p) {
 size_t Pool::slot_bytes(const Problem &p) {
     size_t N = (size_t)p.g.domain_size, A = octahedron_cells(p);
     size_t multilayer = p.cfg.number_of_layers > 1 ? N * 8 : 0;
-    return N * (1 + 4 + 4 + 1 + 4) + A * (4 + 12 + 104 + 8 + 4) + multilayer + p.nuclei_loc.size() * 8 + 64 * 1024;
+    size_t classes = p.du_values.size() > 1 ? N * 2 : 0;
+    return N * (1 + 4 + 4 + 1 + 4) + A * (4 + 12 + 104 + 8 + 4) + multilayer + classes + p.nuclei_loc.size() * 8 +
+           64 * 1024;
 }
 
 Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
@@ -1724,11 +1731,20 @@ void Pool::ensure_growth(int slot, long long needed) {
     long long len = std::max<long long>(needed + 1, std::max<long long>(2LL * s.growth_len, 4096));
     if (len > INT_MAX / 2)
         throw Unsupported("growth table too long");
-    std::vector<double> g;
-    build_growth_table(*s.problem, (int)len, g);
+    // one table per distinct UndercoolingChange value, table c at c * len
+    const Problem &p = *s.problem;
+    const size_t n_tables = std::max<size_t>(1, p.du_values.size());
+    std::vector<double> g(n_tables * (size_t)len);
+    if (p.du_values.size() > 1) {
+        for (size_t c = 0; c < n_tables; c++)
+            build_growth_table(p, p.du_values[c], (int)len, g.data() + c * (size_t)len);
+    }
+    else {
+        build_growth_table(p, p.du_value, (int)len, g.data());
+    }
     double *d = nullptr;
-    CUDA_OK(cudaMalloc(&d, len * sizeof(double)));
-    CUDA_OK(cudaMemcpyAsync(d, g.data(), len * sizeof(double), cudaMemcpyHostToDevice, S(stream_)));
+    CUDA_OK(cudaMalloc(&d, g.size() * sizeof(double)));
+    CUDA_OK(cudaMemcpyAsync(d, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice, S(stream_)));
     if (s.growth) {
         // the old table may still be read by queued work
         CUDA_OK(cudaStreamSynchronize(S(stream_)));
@@ -1774,9 +1790,11 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     const Geometry &g = p.g;
     const int n_layers = p.cfg.number_of_layers;
     const bool multilayer = n_layers > 1;
-    if (multilayer && check_mode)
-        throw Unsupported("device-side termination is not offered for multilayer problems (the layer change "
-                          "runs between launches): admit with device_check 0 and run the plain path");
+    const bool classes = p.du_values.size() > 1;
+    if (check_mode && p.cfg.simulation_type != "C")
+        throw Unsupported("device-side termination covers type-C problems (types S and R jump cycles, stop at "
+                          "finish time steps or change layers between launches): admit with device_check 0 "
+                          "and run the plain path");
     const size_t N = g.domain_size, A = octahedron_cells(p), P = p.nuclei_loc.size();
     // every field of the slot in one allocation (256-byte aligned sub-arrays)
     size_t off = 0;
@@ -1788,7 +1806,8 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     const size_t o_ct = carve(N), o_gid = carve(N * 4), o_cts = carve(N * 4), o_ly = carve(N), o_du = carve(N * 4),
                  o_dl = carve(A * 4), o_doc = carve(A * 12), o_cdl = carve(A * 104), o_claim = carve(A * 8),
                  o_pos = carve(A * 4), o_nl = carve(P * 4), o_nt = carve(P * 4),
-                 o_run = multilayer ? carve(N * 4) : 0, o_base = multilayer ? carve(N * 4) : 0;
+                 o_run = multilayer ? carve(N * 4) : 0, o_base = multilayer ? carve(N * 4) : 0,
+                 o_cls = classes ? carve(N * 2) : 0;
     char *slab = nullptr;
     CUDA_OK(cudaMalloc(&slab, off));
     s.allocs.push_back(slab);
@@ -1807,6 +1826,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     d.pos = (unsigned int *)(slab + o_pos);
     d.cts_run = multilayer ? (int32_t *)(slab + o_run) : d.cts;
     d.nu_base = multilayer ? (int32_t *)(slab + o_base) : nullptr;
+    d.du_class = classes ? (const uint16_t *)(slab + o_cls) : nullptr;
     int32_t *dnl = (int32_t *)(slab + o_nl);
     int32_t *dnt = (int32_t *)(slab + o_nt);
     // nuclei in time order; ties keep the reference's order (order does not change results)
@@ -1830,6 +1850,8 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     CUDA_OK(cudaMemsetAsync(d.pos, 0xff, A * 4, st)); // kNoRecord
     if (multilayer)
         CUDA_OK(cudaMemsetAsync(d.nu_base, 0, N * 4, st));
+    if (classes)
+        CUDA_OK(cudaMemcpyAsync((void *)d.du_class, p.du_class.data(), N * 2, cudaMemcpyHostToDevice, st));
     if (P) {
         CUDA_OK(cudaMemcpyAsync(dnl, nl.data(), P * 4, cudaMemcpyHostToDevice, st));
         CUDA_OK(cudaMemcpyAsync(dnt, nt.data(), P * 4, cudaMemcpyHostToDevice, st));
@@ -1871,12 +1893,14 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     if (multilayer) {
         k_layer_gate<<<num_sms_ * 4, 256, 0, st>>>(ddesc_ + slot);
         CUDA_OK(cudaGetLastError());
+    }
+    if (multilayer || classes) {
         static const int one = 1;
-        CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, multilayer), &one, sizeof(int),
+        CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, extras), &one, sizeof(int),
                                 cudaMemcpyHostToDevice, st));
     }
     ensure_growth(slot, 4096);
-    if (!p.voronoi_seeds.empty() || p.cfg.simulation_type == "S") {
+    if (!p.voronoi_seeds.empty() || p.cfg.simulation_type != "C") {
         int nseeds = (int)(p.voronoi_seeds.size() / 3);
         int32_t *dseeds = nullptr;
         if (nseeds) {
@@ -2359,7 +2383,8 @@ void Pool::copy_out(int slot, int32_t *grain_id, int32_t *cell_type) {
 int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_s) {
     // src/runCA.cpp:282-411: the layer loop, each layer's cycles until no liquid of the layer is left
     const Problem &p = *slots_.at(slot).problem;
-    bool jump_type = p.cfg.simulation_type == "S" || p.cfg.simulation_type == "R";
+    const bool type_r = p.cfg.simulation_type == "R";
+    const bool jump_type = p.cfg.simulation_type == "S" || type_r;
     auto t0 = std::chrono::steady_clock::now();
     auto t_layer = t0;
     cudaEvent_t ev0, ev1;
@@ -2386,7 +2411,20 @@ int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_
           << " Undercooled liquid cells = " << c.undercooled << " Number of nucleation events this layer " << d.nn
           << " Remaining liquid cells in future layers of this simulation = " << c.remaining << "\n";
         log += s.str();
-        if (c.superheated + c.undercooled == 0) {
+        bool xswitch = c.superheated + c.undercooled == 0;
+        if (!xswitch && jump_type && c.undercooled == 0) {
+            unsigned long long next = c.next_cts;
+            if ((next - (unsigned long long)(long long)cycle) > 5000) {
+                int nc = (int)(next - 1);
+                set_cycle(slot, nc);
+                cycle = nc;
+                log += "Jumping to cycle " + std::to_string(cycle + 1) + "\n";
+            }
+            // type R ends a layer at its finish time step (src/CAupdate.cpp:818-819)
+            if (type_r && cycle >= p.finish_time_step.at(d.layer_no))
+                xswitch = true;
+        }
+        if (xswitch) {
             if (d.layer_no + 1 >= d.n_layers)
                 break;
             const int layer = d.layer_no;
@@ -2398,15 +2436,6 @@ int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_
             log += s2.str();
             cycle = 0;
             continue;
-        }
-        if (jump_type && c.undercooled == 0) {
-            unsigned long long next = c.next_cts;
-            if ((next - (unsigned long long)(long long)cycle) > 5000) {
-                int nc = (int)(next - 1);
-                set_cycle(slot, nc);
-                cycle = nc;
-                log += "Jumping to cycle " + std::to_string(cycle + 1) + "\n";
-            }
         }
     }
     CUDA_OK(cudaEventRecord(ev1, S(stream_)));

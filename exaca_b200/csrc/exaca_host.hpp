@@ -25,7 +25,8 @@ enum CellTypeCode : int8_t {
 
 constexpr int kNumOrientations = 10000; // src/runCA.cpp:133
 
-// A valid input this solver does not handle (problem type R, several layers, substrate files).
+// A valid input this solver does not handle (substrate files, more than 127 layers, more distinct
+// UndercoolingChange values than the growth tables hold).
 struct Unsupported : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
@@ -52,7 +53,7 @@ struct InputConfig {
     double dTN = 0, dTsigma = 0;
     std::string path_to_output, output_file;
     std::string orientation_file; // resolved path
-    // type R (parsed for error parity; the solver rejects R)
+    // type R (temperature data from files)
     double ht_deltax = 0;
     std::string temppath, tempfile;
     int temp_files_in_series = 0;
@@ -105,7 +106,13 @@ struct Problem {
     std::vector<int32_t> nuclei_loc, nuclei_time;
     // interfacial response constants after the dt/dx normalisation of src/runCA.cpp:198-200
     double A_n = 0, B_n = 0, C_n = 0, D_n = 0;
-    float du_value = 0.0f; // the one non-zero UndercoolingChange value of this problem
+    float du_value = 0.0f; // the one non-zero UndercoolingChange value of this problem (C and S; R with one value)
+    // type R: the distinct non-zero UndercoolingChange values (ascending) when there are several, and
+    // per cell the index of its value (0 for cells whose value is 0: their undercooling stays 0)
+    std::vector<float> du_values;
+    std::vector<uint16_t> du_class;
+    // type R: per layer, the cycle at which the layer's temperature data ends (FinishTimeStep)
+    std::vector<int> finish_time_step;
     int possible_nuclei = 0;
     double init_seconds = 0.0;
     // baseplate grain centres (x, y, z triples) for the device Voronoi pass of S problems
@@ -167,6 +174,9 @@ inline int find_it_bounds(int rx, int ry, int mx, int my) {
 
 // Growth-increment table: entry n is the diagonal-length increment of an active cell whose
 // undercooling is the n-fold float sum of du (src/CAupdate.cpp:236-261). Entry 0 is U = 0.
+void build_growth_table(const Problem &p, float du, int n_entries, double *growth);
 void build_growth_table(const Problem &p, int n_entries, std::vector<double> &growth);
+// Most distinct UndercoolingChange values a problem may have (one growth table each).
+constexpr int kMaxUndercoolingValues = 1024;
 
 } // namespace exaca

@@ -9,6 +9,7 @@
 #include "exaca_host.hpp"
 
 #include <algorithm>
+#include <cctype>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -140,14 +141,18 @@ void build_cdl_table(const std::vector<float> &guv, std::vector<float> &table) {
 }
 
 void build_growth_table(const Problem &p, int n_entries, std::vector<double> &growth) {
+    growth.resize(n_entries);
+    build_growth_table(p, p.du_value, n_entries, growth.data());
+}
+
+void build_growth_table(const Problem &p, float du, int n_entries, double *growth) {
     // U after n updates is the n-fold float sum of du (src/CAupdate.cpp:236-237, U starts at 0);
     // the increment is min(0.045, max(0, A U^3 + B U^2 + C U + D)) with U capped at 210
     // (src/CAupdate.cpp:257-261), using this host's pow exactly as the reference does.
-    growth.resize(n_entries);
     float u = 0.0f;
     for (int n = 0; n < n_entries; n++) {
         if (n > 0)
-            u += p.du_value * (1);
+            u += du * (1);
         double LocU = u;
         LocU = std::min(210.0, LocU);
         double V = p.A_n * pow(LocU, 3.0) + p.B_n * pow(LocU, 2.0) + p.C_n * LocU + p.D_n;
@@ -254,6 +259,320 @@ void temp_init_spots(Problem &p, std::string &log) {
             }
         }
     }
+}
+
+// ---- type R: reduced temperature data from files ------------------------------------------------
+
+struct TemperatureData {
+    std::vector<double> raw;        // the stored points, 6 values each: x, y, z, tm, tl, cr (RawData)
+    std::vector<long> first, last;  // per layer: its range of raw
+    std::vector<float> zmin_layer, zmax_layer;
+    float xmin = 1000000.0f, ymin = 1000000.0f, zmin = 1000000.0f;
+    float xmax = -1000000.0f, ymax = -1000000.0f, zmax = -1000000.0f;
+};
+
+// src/CAinitialize.cpp:135-146: the first n-1 comma-separated fields, then the rest of the line
+void split_commas(std::string line, std::vector<std::string> &out) {
+    for (size_t n = 0; n + 1 < out.size(); n++) {
+        size_t pos = line.find(',');
+        out[n] = line.substr(0, pos);
+        line = line.substr(pos + 1, std::string::npos);
+    }
+    out.back() = line;
+}
+
+// src/CAinitialize.cpp:149-175: columns x, y, z, tm, tl (or ts), cr (or r), case-insensitive
+void check_temperature_header(const std::string &line) {
+    std::vector<std::string> v(6);
+    split_commas(line, v);
+    static const std::vector<std::vector<std::string>> expected = {{"x"}, {"y"}, {"z"}, {"tm"}, {"tl", "ts"}, {"r", "cr"}};
+    for (size_t n = 0; n < 6; n++) {
+        std::string val;
+        for (char ch : v[n])
+            if (!std::isspace((unsigned char)ch))
+                val += (char)std::tolower((unsigned char)ch);
+        if (std::find(expected[n].begin(), expected[n].end(), val) == expected[n].end())
+            throw std::runtime_error(expected[n].back() + " not found in temperature file header");
+    }
+}
+
+// src/CAinitialize.cpp:177-187: the first pt.size() values of a data line, as std::stod reads them
+void temperature_point(const std::string &line, std::vector<double> &pt) {
+    std::vector<std::string> v(pt.size());
+    split_commas(line, v);
+    for (size_t n = 0; n < pt.size(); n++)
+        pt[n] = std::stod(v[n]);
+}
+
+std::string dstr(double v) {
+    std::ostringstream s;
+    s << v;
+    return s.str();
+}
+
+// x/y range of the temperature grid one rank reads (src/CAinitialize.cpp:906-923, 1171-1188)
+void read_bounds(const Geometry &g, int ratio, int &lx, int &ly, int &ux, int &uy) {
+    lx = g.xoff <= 2 ? 2 : g.xoff - ((g.xoff - 2) % ratio);
+    ly = g.yoff <= 2 ? 2 : g.yoff - ((g.yoff - 2) % ratio);
+    ux = (g.xoff + g.mx - 1 >= g.nx - 3) ? g.nx - 3 : g.xoff + g.mx - 1 + ratio - ((g.xoff + (g.mx - 1) - 2) % ratio);
+    uy = (g.yoff + g.my - 1 >= g.ny - 3) ? g.ny - 3 : g.yoff + g.my - 1 + ratio - ((g.yoff + (g.my - 1) - 2) % ratio);
+}
+
+// ParallelMeshInit for type R (src/CAinitialize.cpp:747-1003): the domain bounds from every file's
+// points, the decomposition, then the points of this rank's x/y range.
+void mesh_init_reduced(Problem &p, TemperatureData &td, std::string &log) {
+    InputConfig &c = p.cfg;
+    const int nfiles = c.temp_files_in_series, layers = c.number_of_layers;
+    std::vector<std::string> paths(nfiles);
+    for (int i = 1; i <= nfiles; i++)
+        paths[i - 1] = c.temppath + "/" + (nfiles > 1 ? std::to_string(i) + c.tempfile : c.tempfile);
+    const int ratio_read = c.ht_deltax / c.deltax; // truncation, as the reference
+    {
+        std::ifstream f(paths[0]);
+        std::string line;
+        std::getline(f, line);
+        if (line.find("Number of temperature data points") != std::string::npos)
+            throw std::runtime_error("Error: Old header and temperature file format no longer supported");
+    }
+    const int to_read = std::min(layers, nfiles);
+    td.zmin_layer.assign(layers, 0.0f);
+    td.zmax_layer.assign(layers, 0.0f);
+    td.first.assign(layers, 0);
+    td.last.assign(layers, 0);
+    for (int L = 1; L <= to_read; L++) {
+        std::ifstream f(paths[L - 1]);
+        std::string header;
+        std::getline(f, header);
+        check_temperature_header(header);
+        std::vector<double> X, Y, Z, pt(3);
+        while (!f.eof()) {
+            std::string line;
+            std::getline(f, line);
+            if (line.empty())
+                break;
+            temperature_point(line, pt);
+            X.push_back(pt[0]);
+            Y.push_back(pt[1]);
+            Z.push_back(pt[2]);
+        }
+        if (X.empty())
+            throw std::runtime_error("Temperature file " + paths[L - 1] + " holds no data points");
+        double x0 = *std::min_element(X.begin(), X.end()), x1 = *std::max_element(X.begin(), X.end());
+        double y0 = *std::min_element(Y.begin(), Y.end()), y1 = *std::max_element(Y.begin(), Y.end());
+        double z0 = *std::min_element(Z.begin(), Z.end()), z1 = *std::max_element(Z.begin(), Z.end());
+        z0 += c.deltax * c.layer_height * (L - 1);
+        z1 += c.deltax * c.layer_height * (L - 1);
+        if (x0 < td.xmin)
+            td.xmin = x0;
+        if (x1 > td.xmax)
+            td.xmax = x1;
+        if (y0 < td.ymin)
+            td.ymin = y0;
+        if (y1 > td.ymax)
+            td.ymax = y1;
+        if (z0 < td.zmin)
+            td.zmin = z0;
+        if (z1 > td.zmax)
+            td.zmax = z1;
+        td.zmin_layer[L - 1] = z0;
+        td.zmax_layer[L - 1] = z1;
+        log += "Layer = " + std::to_string(L) + " Z Bounds are " + dstr(z0) + " " + dstr(z1) + "\n";
+    }
+    // layers beyond the files repeat them, shifted up by the layer offset
+    for (int L = nfiles; L < layers; L++) {
+        if (nfiles == 1) {
+            td.zmin_layer[L] = td.zmin_layer[L - 1] + c.deltax * c.layer_height;
+            td.zmax_layer[L] = td.zmax_layer[L - 1] + c.deltax * c.layer_height;
+        }
+        else {
+            const int rep = L % nfiles, unit = L / nfiles;
+            td.zmin_layer[L] = td.zmin_layer[rep] + unit * nfiles * c.deltax * c.layer_height;
+            td.zmax_layer[L] = td.zmax_layer[rep] + unit * nfiles * c.deltax * c.layer_height;
+        }
+        td.zmax += c.deltax * c.layer_height;
+    }
+    // wall + solid ring at each x/y side, wall + one row at the bottom, wall at the top
+    c.nx = round((td.xmax - td.xmin) / c.deltax) + 1 + 4;
+    c.ny = round((td.ymax - td.ymin) / c.deltax) + 1 + 4;
+    c.nz = round((td.zmax - td.zmin) / c.deltax) + 1 + 3;
+    log += "Domain size: " + std::to_string(c.nx) + " by " + std::to_string(c.ny) + " by " + std::to_string(c.nz) + "\n";
+    log += "X Limits of domain: " + dstr(td.xmin) + " and " + dstr(td.xmax) + "\n";
+    log += "Y Limits of domain: " + dstr(td.ymin) + " and " + dstr(td.ymax) + "\n";
+    log += "Z Limits of domain: " + dstr(td.zmin) + " and " + dstr(td.zmax) + "\n";
+    log += "================================================================\n";
+    decompose(p, log);
+    int lx, ly, ux, uy;
+    read_bounds(p.g, ratio_read, lx, ly, ux, uy);
+    for (int L = 1; L <= to_read; L++) {
+        std::ifstream f(paths[L - 1]);
+        td.first[L - 1] = (long)td.raw.size();
+        std::string line;
+        std::getline(f, line); // header
+        std::vector<double> pt(6);
+        while (!f.eof()) {
+            std::getline(f, line);
+            if (line.empty())
+                break;
+            temperature_point(line, pt);
+            const int xi = round((pt[0] - td.xmin) / c.deltax) + 2;
+            const int yi = round((pt[1] - td.ymin) / c.deltax) + 2;
+            if (xi >= lx && xi <= ux && yi >= ly && yi <= uy)
+                td.raw.insert(td.raw.end(), pt.begin(), pt.end());
+        }
+        td.last[L - 1] = (long)td.raw.size();
+    }
+    for (int L = nfiles; L < layers; L++) {
+        const int from = nfiles == 1 ? L - 1 : L % nfiles;
+        td.first[L] = td.first[from];
+        td.last[L] = td.last[from];
+    }
+}
+
+// TempInit_Reduced (src/CAinitialize.cpp:1128-1405): per layer, the last liquidus time and the
+// cooling rate of every temperature point, trilinear interpolation onto the CA grid when the
+// temperature grid is coarser, then CritTimeStep, UndercoolingChange, LayerID and Melted of the
+// cells whose normalised liquidus time is positive, and the layer's finish time step.
+void temp_init_reduced(Problem &p, const TemperatureData &td, std::string &log) {
+    InputConfig &c = p.cfg;
+    Geometry &g = p.g;
+    const double unrounded = c.ht_deltax / c.deltax, fl = floor(unrounded);
+    if (unrounded - fl > 0.0005)
+        throw std::runtime_error("Error: Temperature data point spacing not evenly divisible by CA cell size");
+    else if (unrounded - fl > 0.000001)
+        log += "Note: Adjusting cell size from " + dstr(c.deltax) + " to " + dstr(c.ht_deltax / fl) +
+               " to ensure even divisibility of CA cell size into temperature data spacing\n";
+    c.deltax = c.ht_deltax / fl;
+    const int ratio = round(c.ht_deltax / c.deltax);
+    int lx, ly, ux, uy;
+    read_bounds(g, ratio, lx, ly, ux, uy);
+    for (long i = 0; i < g.domain_size; i++) {
+        p.melted[i] = 0;
+        p.layer_id[i] = -1;
+    }
+    const int layers = c.number_of_layers;
+    p.finish_time_step.assign(layers, 0);
+    const int sx = ux - lx + 1, sy = uy - ly + 1;
+    for (int L = 0; L < layers; L++) {
+        double smallest = 1000000000, largest = 0;
+        const int nzt = round((td.zmax_layer[L] - td.zmin_layer[L]) / c.deltax) + 1;
+        log += "Initializing temporary temperature data structures with " + std::to_string(nzt) +
+               " cells in z direction\n";
+        log += "Layer " + std::to_string(L) + " rank 0 ZMin this layer is " + dstr(td.zmin_layer[L]) + "\n";
+        std::vector<double> CR((size_t)nzt * sx * sy, -1.0), TL((size_t)nzt * sx * sy, -1.0);
+        auto at = [&](int z, int x, int y) -> size_t {
+            if (z < 0 || z >= nzt || x < 0 || x >= sx || y < 0 || y >= sy)
+                throw std::runtime_error("temperature data point outside the layer's temperature grid");
+            return ((size_t)z * sx + x) * sy + y;
+        };
+        const long start = td.first[L], end = td.last[L];
+        log += "Range for layer " + std::to_string(L) + " on rank 0 is " + std::to_string(start) + " to " +
+               std::to_string(end) + "\n";
+        int xi = -1, yi = -1, zi = -1;
+        for (long i = start; i < end; i++) {
+            const int pos = (int)(i % 6);
+            if (pos == 0) {
+                xi = round((td.raw[i] - td.xmin) / c.deltax) + 2;
+            }
+            else if (pos == 1) {
+                yi = round((td.raw[i] - td.ymin) / c.deltax) + 2;
+            }
+            else if (pos == 2) {
+                zi = round((td.raw[i] + c.deltax * c.layer_height * L - td.zmin_layer[L]) / c.deltax);
+            }
+            else if (pos == 4) {
+                // only the last time the point goes below the liquidus counts
+                const size_t q = at(zi, xi - lx, yi - ly);
+                if (td.raw[i] > TL[q]) {
+                    TL[q] = td.raw[i];
+                    if (td.raw[i] < smallest)
+                        smallest = td.raw[i];
+                }
+                else {
+                    i = i + 1; // skip this point's cooling rate
+                }
+            }
+            else if (pos == 5) {
+                const size_t q = at(zi, xi - lx, yi - ly);
+                CR[q] = td.raw[i];
+                float solidus = TL[q] + c.freezing_range / CR[q];
+                if (solidus > largest)
+                    largest = solidus;
+            }
+        }
+        log += "Smallest time globally for layer " + std::to_string(L) + " is " + dstr(smallest) + "\n";
+        log += "Largest time globally for layer " + std::to_string(L) + " is " + dstr(largest) + "\n";
+        p.finish_time_step[L] = round((largest - smallest) / c.deltat);
+        log += " Layer " + std::to_string(L) + " FINISH TIME STEP IS " + std::to_string(p.finish_time_step[L]) + "\n";
+        log += "Layer " + std::to_string(L) + " temperatures read\n";
+        if (ratio != 1) {
+            // in place, in the reference's loop order (later cells may read interpolated values)
+            for (int k = 0; k < nzt; k++) {
+                const int lowz = k - (k % ratio);
+                int highz = lowz + ratio;
+                const double fhz = (double)(k - lowz) / (double)(ratio), flz = 1.0 - fhz;
+                if (highz > nzt - 1)
+                    highz = lowz;
+                for (int i = 0; i <= ux - lx; i++) {
+                    const int lowx = i - (i % ratio);
+                    int highx = lowx + ratio;
+                    const double fhx = (double)(i - lowx) / (double)(ratio), flx = 1.0 - fhx;
+                    if (highx >= ux - lx)
+                        highx = ux - lx;
+                    for (int j = 0; j <= uy - ly; j++) {
+                        const int lowy = j - (j % ratio);
+                        int highy = lowy + ratio;
+                        const double fhy = (float)(j - lowy) / (float)(ratio), fly = 1.0 - fhy;
+                        if (highy >= uy - ly)
+                            highy = uy - ly;
+                        for (std::vector<double> *F : {&TL, &CR}) {
+                            std::vector<double> &A = *F;
+                            const double p1 = A[at(lowz, lowx, lowy)], p2 = A[at(lowz, highx, lowy)];
+                            const double p12 = flx * p1 + fhx * p2;
+                            const double p3 = A[at(lowz, lowx, highy)], p4 = A[at(lowz, highx, highy)];
+                            const double p34 = flx * p3 + fhx * p4;
+                            const double p1234 = p12 * fly + p34 * fhy;
+                            const double p5 = A[at(highz, lowx, lowy)], p6 = A[at(highz, highx, lowy)];
+                            const double p56 = flx * p5 + fhx * p6;
+                            const double p7 = A[at(highz, lowx, highy)], p8 = A[at(highz, highx, highy)];
+                            const double p78 = flx * p7 + fhx * p8;
+                            const double p5678 = p56 * fly + p78 * fhy;
+                            if (p1 > 0 && p2 > 0 && p3 > 0 && p4 > 0 && p5 > 0 && p6 > 0 && p7 > 0 && p8 > 0)
+                                A[at(k, i, j)] = p1234 * flz + p5678 * fhz;
+                        }
+                    }
+                }
+            }
+        }
+        log += "Interpolation done\n";
+        const int zbase = round((td.zmin_layer[L] - td.zmin) / c.deltax) + 2;
+        if (L == 0) {
+            g.zbound_low = 0;
+            g.zbound_high = zbase + nzt - 1;
+            g.nz_active = g.zbound_high - g.zbound_low + 1;
+        }
+        log += "Layer " + std::to_string(L) + " data belongs to global z coordinates of " + std::to_string(zbase) +
+               " through " + std::to_string(zbase + nzt - 1) + "\n";
+        for (int k = 0; k < nzt; k++)
+            for (int ii = lx; ii <= ux; ii++)
+                for (int jj = ly; jj <= uy; jj++) {
+                    if (ii < g.xoff || ii >= g.xoff + g.mx || jj < g.yoff || jj >= g.yoff + g.my)
+                        continue;
+                    const size_t q = at(k, ii - lx, jj - ly);
+                    // liquidus time from the start of the layer
+                    const double ctl = TL[q] - smallest;
+                    if (ctl > 0) {
+                        const int z = zbase + k;
+                        if (z < 0 || z >= g.nz)
+                            throw std::runtime_error("temperature data outside the domain in z");
+                        const long idx = (long)z * g.mx * g.my + (long)(ii - g.xoff) * g.my + (jj - g.yoff);
+                        p.melted[idx] = 1;
+                        p.cts[idx] = round(ctl / c.deltat);
+                        p.layer_id[idx] = L;
+                        p.du[idx] = std::abs(CR[q]) * c.deltat;
+                    }
+                }
+    }
+    log += "First layer Z bounds are " + std::to_string(g.zbound_low) + " and " + std::to_string(g.zbound_high) + "\n";
 }
 
 // src/CAinitialize.cpp:1460-1529 (np = 1: rank seed 0, grain IDs 1, 2, ... in index order)
@@ -450,22 +769,27 @@ void nuclei_init(Problem &p, std::string &log) {
 void initialize_problem(Problem &p, std::string &log) {
     auto t0 = std::chrono::steady_clock::now();
     InputConfig &c = p.cfg;
-    if (c.simulation_type == "R")
-        throw Unsupported("Problem type R (temperature data from files) is not supported by the B200 solver");
-    if (c.simulation_type != "C" && c.simulation_type != "S")
+    const bool type_r = c.simulation_type == "R";
+    if (c.simulation_type != "C" && c.simulation_type != "S" && !type_r)
         throw std::runtime_error("Unknown problem type \"" + c.simulation_type + "\"");
     if (c.number_of_layers < 1 || c.number_of_layers > 127)
         throw Unsupported("Number of layers must be between 1 and 127 (LayerID is stored in 8 bits)");
-    if (c.simulation_type == "S" && c.use_substrate_file)
+    if (c.simulation_type != "C" && c.use_substrate_file)
         throw Unsupported("Substrate files are not supported by the B200 solver");
 
     int it[9][26], lens[9];
     build_itlist(it, lens);
-    decompose(p, log);
+    TemperatureData td;
+    if (type_r) {
+        mesh_init_reduced(p, td, log);
+    }
+    else {
+        decompose(p, log);
+        log += "Constrained solidification domain size: " + std::to_string(p.g.nx) + " by " +
+               std::to_string(p.g.ny) + " by " + std::to_string(p.g.nz) + "\n";
+        log += "================================================================\n";
+    }
     Geometry &g = p.g;
-    log += "Constrained solidification domain size: " + std::to_string(g.nx) + " by " + std::to_string(g.ny) +
-           " by " + std::to_string(g.nz) + "\n";
-    log += "================================================================\n";
     log += "Mesh initialized\n";
     if ((long)g.mx * g.my * g.nz > 2000000000L)
         throw Unsupported("domain too large: the cell index must fit in 31 bits");
@@ -479,8 +803,11 @@ void initialize_problem(Problem &p, std::string &log) {
 
     if (c.simulation_type == "C")
         temp_init_directional(p);
+    else if (type_r)
+        temp_init_reduced(p, td, log);
     else
         temp_init_spots(p, log);
+    td = TemperatureData(); // the raw temperature points are not needed past this point
     g.active_size = (long)g.mx * g.my * g.nz_active;
     log += "Done with temperature field initialization, active domain size is " + std::to_string(g.nz_active) +
            " out of " + std::to_string(g.nz) + " cells in the Z direction\n";
@@ -509,18 +836,28 @@ void initialize_problem(Problem &p, std::string &log) {
     p.C_n = c.C * c.deltat / c.deltax;
     p.D_n = c.D;
 
-    // The device growth model needs every cell's UndercoolingChange to be 0 or one common value.
-    float common = 0.0f;
-    for (long i = 0; i < g.domain_size; i++) {
-        float v = p.du[i];
-        if (v == 0.0f)
-            continue;
-        if (common == 0.0f)
-            common = v;
-        else if (v != common)
-            throw Unsupported("non-uniform UndercoolingChange is not supported by the B200 solver");
+    // The device growth model reads one growth table per distinct non-zero UndercoolingChange value
+    // (types C and S have one; type R one per cooling rate after interpolation).
+    std::vector<float> values;
+    for (long i = 0; i < g.domain_size; i++)
+        if (p.du[i] != 0.0f)
+            values.push_back(p.du[i]);
+    std::sort(values.begin(), values.end());
+    values.erase(std::unique(values.begin(), values.end()), values.end());
+    if ((int)values.size() > kMaxUndercoolingValues)
+        throw Unsupported("the temperature data give " + std::to_string(values.size()) +
+                          " distinct UndercoolingChange values; the B200 solver holds at most " +
+                          std::to_string(kMaxUndercoolingValues) + " growth tables");
+    p.du_value = values.empty() ? 0.0f : values[0];
+    p.du_values.clear();
+    p.du_class.clear();
+    if (values.size() > 1) {
+        p.du_values = values;
+        p.du_class.assign(g.domain_size, 0);
+        for (long i = 0; i < g.domain_size; i++)
+            if (p.du[i] != 0.0f)
+                p.du_class[i] = (uint16_t)(std::lower_bound(values.begin(), values.end(), p.du[i]) - values.begin());
     }
-    p.du_value = common;
     p.voronoi_seeds = seeds;
     p.init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
 }

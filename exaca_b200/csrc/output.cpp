@@ -330,6 +330,18 @@ void write_log(const Problem &p, const std::string &fname, int cycle, const RunT
           << " microns" << "\n";
         L << "This pattern was repeated for " << c.number_of_layers << " layers" << "\n";
     }
+    else {
+        L << c.number_of_layers << " layers were simulated, with an offset of " << c.layer_height << " cells" << "\n";
+        L << (c.remelting ? "Remelting was included" : "Remelting was not included") << "\n";
+        if (c.use_substrate_file)
+            L << "The substrate file was " << c.substrate_file_name << "\n";
+        else
+            L << "The mean substrate grain size was " << c.substrate_grain_spacing << " microns" << "\n";
+        if (c.simulation_type == "R") {
+            L << "The " << c.temp_files_in_series << " temperature file(s) used had the name " << c.tempfile << "\n";
+            L << "The temperature data resolution was " << c.ht_deltax << " microns" << "\n";
+        }
+    }
     L << "The decomposition scheme used was: " << c.decomposition_strategy << "\n";
     L << "Rank " << 0 << " contained " << g.mx << " cells in x , " << g.my << " cells in y; subdomain was offset by "
       << g.xoff << " in x , " << g.yoff << " in y" << "\n";

@@ -103,6 +103,9 @@ struct DomainDesc {
     // single-layer problems cts_run == cts and nu_base is null.
     int32_t *cts_run;
     int32_t *nu_base;
+    // Several UndercoolingChange values (type R): per cell the index of its growth table, which is
+    // table du_class[cell] of growth (growth_len entries each). Null with one value.
+    const uint16_t *du_class;
     int layer_no;
     int n_layers;
     int z_lo, z_end;
@@ -135,7 +138,7 @@ struct PoolState {
     int compact;              // 1: this cycle's growth pass writes the survivors to list cur ^ 1
     int error;
     int n_domains;
-    int multilayer; // 1 once a multilayer domain was admitted (its records carry earlier layers' updates)
+    int extras; // 1 once a domain with per-cell growth extras (several layers or undercooling values) was admitted
     DomainDesc *desc;
     unsigned long long stat[kStatShards][kNumStats];
     unsigned int blocks_done;      // last-block detection of the separate capture kernel

@@ -41,6 +41,10 @@ def debug_variant(src, dst, outdir):
             ln = "Path to output: " + outdir + "/"
         if "Print data for main Kokkos views" in ln or "Print data for all main data structures" in ln:
             ln = ln[: ln.rfind(":") + 1] + " Y"
+        if ln.startswith("Path to temperature file"):
+            # relative to tests/golden/inputs (the reference resolves it against its working directory)
+            key, rel = ln.split(":", 1)
+            ln = key + ": " + os.path.join(INPUTS, rel.strip())
         out.append(ln)
     open(dst, "w").write("\n".join(out) + "\n")
 

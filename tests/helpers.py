@@ -1,5 +1,6 @@
 """Shared helpers of the parity tests (test infrastructure)."""
 import os
+import tempfile
 
 import numpy as np
 
@@ -16,8 +17,23 @@ def load_golden(case):
     return np.load(os.path.join(GOLDEN, case + ".npz"))
 
 
+def resolve_temperature_path(line):
+    """Temperature-file paths of the golden inputs are relative to tests/golden/inputs; the solver
+    (like the reference) resolves them against the working directory, so copies get absolute ones."""
+    if line.startswith("Path to temperature file"):
+        key, rel = line.split(":", 1)
+        return key + ": " + os.path.join(INPUTS, rel.strip())
+    return line
+
+
 def input_path(case):
-    return os.path.join(INPUTS, case + ".txt")
+    src = os.path.join(INPUTS, case + ".txt")
+    lines = open(src).read().splitlines()
+    if not any(ln.startswith("Path to temperature file") for ln in lines):
+        return src
+    dst = os.path.join(tempfile.gettempdir(), f"exaca_golden_{os.getpid()}_{case}.txt")
+    open(dst, "w").write("\n".join(resolve_temperature_path(ln) for ln in lines) + "\n")
+    return dst
 
 
 def to_whole(a, shape):
@@ -37,7 +53,7 @@ def copy_input(case, outdir):
     for ln in lines:
         if ln.startswith("Path to output"):
             ln = "Path to output: " + outdir + "/"
-        out.append(ln)
+        out.append(resolve_temperature_path(ln))
     dst = os.path.join(outdir, case + ".txt")
     open(dst, "w").write("\n".join(out) + "\n")
     return dst
