@@ -432,41 +432,51 @@ __device__ __noinline__ void begin_domains(PoolState *P, int first_warp, int war
     const int cur = P->cur;
     const int lane = threadIdx.x & 31;
     unsigned long long nucleated = 0;
-    for (int d = first_warp; d < P->n_domains; d += warp_stride) {
-        DomainDesc &D = P->desc[d];
-        if (D.ctype == nullptr || D.done)
+    const int n_domains = P->n_domains;
+    DomainDesc *const desc = P->desc;
+    for (int d = first_warp; d < n_domains; d += warp_stride) {
+        DomainDesc &D = desc[d];
+        // Every field the start reads, and the first 32 nuclei from the cursor, in one round of
+        // loads: this runs while the rest of the grid waits, so its dependent chain is the cost.
+        const int8_t *const ctype = D.ctype;
+        const int done = D.done, check_mode = D.check_mode, cycle0 = D.cycle, cursor0 = D.nuc_cursor;
+        const int n_nuclei = D.n_nuclei, layer_no = D.layer_no, nn0 = D.nn;
+        const unsigned int epoch0 = D.epoch;
+        const long long liquid0 = D.liquid, active_size = D.active_size;
+        const int32_t *const nuc_time = D.nuc_time, *const nuc_loc = D.nuc_loc;
+        if (ctype == nullptr || done)
             continue;
-        if (D.check_mode && D.cycle > 0 && D.cycle % 1000 == 0 && domain_liquid(D) == 0) {
+        int idx = cursor0 + lane;
+        int t = idx < n_nuclei ? __ldg(nuc_time + idx) : INT_MAX;
+        int l = idx < n_nuclei ? __ldg(nuc_loc + idx) : -1;
+        __syncwarp(); // every lane has read the cycle before lane 0 advances it
+        if (check_mode && cycle0 > 0 && cycle0 % 1000 == 0 && domain_liquid(D) == 0) {
             // src/CAupdate.cpp:782-783: no superheated or undercooled liquid left
             if (lane == 0)
                 D.done = 1;
             continue;
         }
-        const int cycle = D.cycle + 1;
-        __syncwarp();
+        const int cycle = cycle0 + 1;
         if (lane == 0) {
             D.cycle = cycle;
-            D.epoch = D.epoch + 1;
+            D.epoch = epoch0 + 1;
         }
         // src/CAupdate.cpp:76-198: sites with cycle >= NucleationTimes that are still liquid
-        int cursor = D.nuc_cursor;
+        int cursor = cursor0;
         int fired_total = 0;
-        while (cursor < D.n_nuclei) {
-            int idx = cursor + lane;
-            int t = idx < D.n_nuclei ? D.nuc_time[idx] : INT_MAX;
+        while (true) {
             unsigned int due = __ballot_sync(0xffffffffu, t <= cycle);
             // nuclei are sorted by time, so the due ones form a prefix
             int n_due = __popc(due);
             bool fire = false;
             unsigned int loc = 0;
             if (t <= cycle) {
-                int l = D.nuc_loc[idx];
-                if (l < 0 || l >= D.active_size) {
+                if (l < 0 || l >= active_size) {
                     atomicOr(&D.error, kErrBounds);
                 }
                 else {
                     loc = (unsigned int)l;
-                    fire = __ldcg(D.ctype + loc) == kLiquid && D.layer[loc] <= D.layer_no;
+                    fire = __ldcg(ctype + loc) == kLiquid && D.layer[loc] <= layer_no;
                 }
             }
             if (fire) {
@@ -492,13 +502,16 @@ __device__ __noinline__ void begin_domains(PoolState *P, int first_warp, int war
             unsigned int fired = __ballot_sync(0xffffffffu, fire);
             fired_total += __popc(fired);
             cursor += n_due;
-            if (n_due < 32)
+            if (n_due < 32 || cursor >= n_nuclei)
                 break;
+            idx = cursor + lane;
+            t = idx < n_nuclei ? __ldg(nuc_time + idx) : INT_MAX;
+            l = idx < n_nuclei ? __ldg(nuc_loc + idx) : -1;
         }
         if (lane == 0) {
             D.nuc_cursor = cursor;
-            D.nn += fired_total;
-            D.liquid -= fired_total;
+            D.nn = nn0 + fired_total;
+            D.liquid = liquid0 - fired_total;
             nucleated += fired_total;
         }
     }
