@@ -10,9 +10,10 @@ the reference seeds it).
 
 metric: cell-updates/s = active-window cells x CA cycles executed / solve time (the reference's
 per-cycle sweep size times cycles). `value` is timed with CUDA events around each solve with the
-initial state already resident in HBM; `e2e` times the same solve through the C ABI from pinned host
-buffers (admission upload + solve + GrainID/CellType download). The state (~20 GB) is larger than
-L2 and is re-uploaded between steps.
+initial state already resident in HBM; `e2e` times the same solve through the C ABI (admission:
+upload of the seeds the cell fields are made from on the device, the fields' construction, the
+solve, and the GrainID/CellType download into pinned host buffers). The state (~20 GB) is larger
+than L2 and is rebuilt between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size S]
 
@@ -265,6 +266,7 @@ def b200_arm(args, rank, world, local):
     ct = torch.empty(g.domain_size, dtype=torch.int32, pin_memory=True)
     lib = ex.load_library()
     barrier()
+    se0 = pool.stats()
     t_e = time.perf_counter()
     slot = pool.admit(prob, device_check=False)
     c_e = pool.run_plain(slot)
@@ -274,8 +276,11 @@ def b200_arm(args, rank, world, local):
         raise RuntimeError(lib.exaca_last_error())
     pool.retire(slot)
     e2e_s = max_over_ranks(e2e_s)
-    h2d = g.domain_size * (1 + 4 + 4 + 1 + 4) + 8 * g.n_nuclei
-    d2h = 8 * g.domain_size
+    se1 = pool.stats()
+    # the bytes the pool copied: the substrate seeds, plane CritTimeSteps and nuclei the cell fields
+    # are made from on the device, the growth tables as the solve lengthens, GrainID and CellType back
+    h2d = se1["h2d_bytes"] - se0["h2d_bytes"]
+    d2h = se1["d2h_bytes"] - se0["d2h_bytes"]
     e2e_value = world * cells * c_e / e2e_s
 
     # roofline of the persistent kernel (k_cycles, the only kernel of the timed solve apart from

@@ -75,7 +75,7 @@ class DomainStatus(ctypes.Structure):
 class PoolStatsT(ctypes.Structure):
     _fields_ = [(n, ctypes.c_uint64) for n in
                 ("cycles", "launches", "listed", "grown", "captured", "nucleated", "claims", "row_reads", "dropped",
-                 "fresh", "rechecks", "flagged")]
+                 "fresh", "rechecks", "flagged", "h2d_bytes", "d2h_bytes")]
 
 
 class CensusT(ctypes.Structure):

@@ -180,6 +180,9 @@ int exaca_problem_fields(const exaca_problem *p, int32_t *cell_type, int32_t *gr
     if (!p)
         return fail(EXACA_ERR_ARG, "null argument");
     const exaca::Problem &q = *p->p;
+    int rc = guarded([&] { exaca::materialize_fields(q); });
+    if (rc != EXACA_OK)
+        return rc;
     long n = q.g.domain_size;
     for (long i = 0; i < n; i++) {
         if (cell_type)
@@ -301,6 +304,8 @@ int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st) {
         st->fresh = s.fresh;
         st->rechecks = s.rechecks;
         st->flagged = s.flagged;
+        st->h2d_bytes = s.h2d_bytes;
+        st->d2h_bytes = s.d2h_bytes;
     });
 }
 
@@ -490,6 +495,7 @@ int exaca_run_program(const char *input_file, int device) {
         if (p->cfg.print_debug) {
             std::vector<int32_t> gid(g.domain_size);
             pool.copy_out(slot, gid.data(), nullptr);
+            exaca::materialize_fields(*p);
             exaca::Problem dbg = *p;
             dbg.grain_id = gid;
             log += "Printing initial data structures to a vtk file " + prefix + "_debug.vtk for debugging\n";

@@ -1468,6 +1468,40 @@ __global__ void k_flush_records(PoolState *P) {
 }
 
 // ---------------------------------------------------------------------------------------------
+// Cell fields of a type-C problem made on the device (src/CAinitialize.cpp:1025-1055, 1460-1529,
+// 1834-2247): walls on the ghost ring and the bottom and top planes, liquid elsewhere, the plane's
+// CritTimeStep, LayerID 0, one UndercoolingChange value; then the substrate seeds (active, GrainID
+// rank + 1) and the nuclei (GrainID -(rank + 1), in index order).
+__global__ void k_fill_directional(int8_t *ctype, int32_t *gid, int32_t *cts, int8_t *layer, float *du, long long n,
+                                   int mx, int my, int nz, const int32_t *plane_cts, float du_value) {
+    const long long plane = (long long)mx * my;
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(c / plane);
+        const int rem = (int)(c - (long long)k * plane);
+        const int i = rem / my, j = rem - (rem / my) * my;
+        const bool wall = i == 0 || i == mx - 1 || j == 0 || j == my - 1 || k == 0 || k == nz - 1;
+        ctype[c] = wall ? kWall : kLiquid;
+        gid[c] = 0;
+        cts[c] = __ldg(plane_cts + k);
+        layer[c] = 0;
+        du[c] = du_value;
+    }
+}
+
+__global__ void k_scatter_seeds(int8_t *ctype, int32_t *gid, const long long *active, long long n_active,
+                                const int32_t *nuclei, long long n_nuclei) {
+    const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (q < n_active) {
+        ctype[active[q]] = kActive;
+        gid[active[q]] = (int32_t)(q + 1);
+    }
+    else if (q < n_active + n_nuclei) {
+        const long long r = q - n_active;
+        gid[nuclei[r]] = -(int32_t)(r + 1);
+    }
+}
+
+// ---------------------------------------------------------------------------------------------
 // Layer change of a multilayer domain (src/runCA.cpp:344-411).
 
 // Undercooling updates of the ending layer, carried into the next: every liquid or active cell of
@@ -1646,6 +1680,16 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
     grid_claim_ = num_sms_ * std::max(b, 1);
     if (const char *m = std::getenv("EXACA_STEP_MODE"))
         step_mode_ = std::string(m) == "graph" ? 1 : 0;
+    {
+        // Domain slabs and growth tables come from the device's stream-ordered pool: admission and
+        // retirement then queue behind running cycles instead of synchronising the device, and
+        // freed slabs are reused by later admissions (the pool keeps what it has reserved until
+        // this process ends).
+        cudaMemPool_t mp;
+        CUDA_OK(cudaDeviceGetDefaultMemPool(&mp, device));
+        unsigned long long keep = ~0ull;
+        CUDA_OK(cudaMemPoolSetAttribute(mp, cudaMemPoolAttrReleaseThreshold, &keep));
+    }
     CUDA_OK(cudaMalloc(&dstate_, sizeof(PoolState)));
     CUDA_OK(cudaMalloc(&ddesc_, sizeof(DomainDesc) * (max_domains_ + 1)));
     CUDA_OK(cudaMemset(ddesc_, 0, sizeof(DomainDesc) * (max_domains_ + 1)));
@@ -1729,6 +1773,7 @@ const DeviceTables &Pool::tables_for(const Problem &p) {
     CUDA_OK(cudaMalloc(&t.cdl_table, p.cdl_table.size() * sizeof(float)));
     CUDA_OK(cudaMemcpy(t.guv, p.guv.data(), p.guv.size() * sizeof(float), cudaMemcpyHostToDevice));
     CUDA_OK(cudaMemcpy(t.cdl_table, p.cdl_table.data(), p.cdl_table.size() * sizeof(float), cudaMemcpyHostToDevice));
+    h2d_bytes_ += (p.guv.size() + p.cdl_table.size()) * sizeof(float);
     return tables_[p.cfg.orientation_file] = t;
 }
 
@@ -1756,12 +1801,12 @@ void Pool::ensure_growth(int slot, long long needed) {
         build_growth_table(p, p.du_value, (int)len, g.data());
     }
     double *d = nullptr;
-    CUDA_OK(cudaMalloc(&d, g.size() * sizeof(double)));
+    CUDA_OK(cudaMallocAsync((void **)&d, g.size() * sizeof(double), S(stream_)));
     CUDA_OK(cudaMemcpyAsync(d, g.data(), g.size() * sizeof(double), cudaMemcpyHostToDevice, S(stream_)));
+    h2d_bytes_ += g.size() * sizeof(double);
     if (s.growth) {
-        // the old table may still be read by queued work
-        CUDA_OK(cudaStreamSynchronize(S(stream_)));
-        CUDA_OK(cudaFree(s.growth));
+        // queued work may still read the old table: it is freed in stream order after that work
+        CUDA_OK(cudaFreeAsync(s.growth, S(stream_)));
     }
     s.growth = d;
     s.growth_len = (int)len;
@@ -1822,7 +1867,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
                  o_run = multilayer ? carve(N * 4) : 0, o_base = multilayer ? carve(N * 4) : 0,
                  o_cls = classes ? carve(N * 2) : 0;
     char *slab = nullptr;
-    CUDA_OK(cudaMalloc(&slab, off));
+    CUDA_OK(cudaMallocAsync((void **)&slab, off, S(stream_)));
     s.allocs.push_back(slab);
     s.bytes = off;
     DomainDesc d;
@@ -1853,11 +1898,43 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     }
     // host->device copies on the pool stream; pageable sources are staged before each call returns
     cudaStream_t st = S(stream_);
-    CUDA_OK(cudaMemcpyAsync(d.ctype, p.cell_type.data(), N, cudaMemcpyHostToDevice, st));
-    CUDA_OK(cudaMemcpyAsync(d.gid, p.grain_id.data(), N * 4, cudaMemcpyHostToDevice, st));
-    CUDA_OK(cudaMemcpyAsync(d.cts, p.cts.data(), N * 4, cudaMemcpyHostToDevice, st));
-    CUDA_OK(cudaMemcpyAsync(d.layer, p.layer_id.data(), N, cudaMemcpyHostToDevice, st));
-    CUDA_OK(cudaMemcpyAsync(d.du, p.du.data(), N * 4, cudaMemcpyHostToDevice, st));
+    if (p.dir.used) {
+        // type C: the cell fields are made here from the plane CritTimeSteps, the substrate seeds and
+        // the nuclei (a few KB cross PCIe instead of 14 bytes per cell)
+        const size_t nk = p.dir.plane_cts.size(), na = p.dir.active.size(), nn = p.nuclei_loc.size();
+        const size_t bytes = nk * 4 + na * 8 + nn * 4;
+        // one upload: the 8-byte seed indices first (the allocation is 256-byte aligned), then the
+        // 4-byte plane CritTimeSteps and nucleus indices
+        std::vector<char> host(bytes);
+        std::memcpy(host.data(), p.dir.active.data(), na * 8);
+        std::memcpy(host.data() + na * 8, p.dir.plane_cts.data(), nk * 4);
+        std::memcpy(host.data() + na * 8 + nk * 4, p.nuclei_loc.data(), nn * 4);
+        char *dseed = nullptr;
+        CUDA_OK(cudaMallocAsync((void **)&dseed, std::max<size_t>(bytes, 16), st));
+        CUDA_OK(cudaMemcpyAsync(dseed, host.data(), bytes, cudaMemcpyHostToDevice, st));
+        h2d_bytes_ += bytes;
+        const long long *active = (const long long *)dseed;
+        const int32_t *plane_cts = (const int32_t *)(dseed + na * 8);
+        const int32_t *nuc = (const int32_t *)(dseed + na * 8 + nk * 4);
+        const unsigned blocks = (unsigned)std::min<long long>((N + 255) / 256, (long long)num_sms_ * 16);
+        k_fill_directional<<<blocks, 256, 0, st>>>(d.ctype, d.gid, d.cts, d.layer, d.du, (long long)N, g.mx, g.my,
+                                                   g.nz, plane_cts, p.du_value);
+        CUDA_OK(cudaGetLastError());
+        const long long nseed = (long long)(na + nn);
+        if (nseed)
+            k_scatter_seeds<<<(unsigned)((nseed + 255) / 256), 256, 0, st>>>(d.ctype, d.gid, active, (long long)na,
+                                                                             nuc, (long long)nn);
+        CUDA_OK(cudaGetLastError());
+        CUDA_OK(cudaFreeAsync(dseed, st));
+    }
+    else {
+        CUDA_OK(cudaMemcpyAsync(d.ctype, p.cell_type.data(), N, cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(d.gid, p.grain_id.data(), N * 4, cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(d.cts, p.cts.data(), N * 4, cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(d.layer, p.layer_id.data(), N, cudaMemcpyHostToDevice, st));
+        CUDA_OK(cudaMemcpyAsync(d.du, p.du.data(), N * 4, cudaMemcpyHostToDevice, st));
+        h2d_bytes_ += N * 14;
+    }
     CUDA_OK(cudaMemsetAsync(d.dl, 0, A * 4, st));
     CUDA_OK(cudaMemsetAsync(d.claim, 0xff, A * 8, st));
     CUDA_OK(cudaMemsetAsync(d.pos, 0xff, A * 4, st)); // kNoRecord
@@ -1869,6 +1946,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
         CUDA_OK(cudaMemcpyAsync(dnl, nl.data(), P * 4, cudaMemcpyHostToDevice, st));
         CUDA_OK(cudaMemcpyAsync(dnt, nt.data(), P * 4, cudaMemcpyHostToDevice, st));
     }
+    h2d_bytes_ += (classes ? N * 2 : 0) + P * 8;
     const DeviceTables &tb = tables_for(p);
     d.guv = tb.guv;
     d.cdl_table = tb.cdl_table;
@@ -1892,12 +1970,19 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     d.du_value = p.du_value;
     long long liquid = 0;
     int zero_du = 0;
-    for (long i = 0; i < g.domain_size; i++) {
-        int8_t t = p.cell_type[i];
-        if (t == kLiquid && p.layer_id[i] == 0)
-            liquid++;
-        if ((t == kLiquid || t == kActive) && p.du[i] == 0.0f)
-            zero_du = 1;
+    if (p.dir.used) {
+        // every cell inside the wall ring is liquid except the substrate seeds
+        liquid = (long long)(g.mx - 2) * (g.my - 2) * (g.nz - 2) - (long long)p.dir.active.size();
+        zero_du = p.du_value == 0.0f ? 1 : 0;
+    }
+    else {
+        for (long i = 0; i < g.domain_size; i++) {
+            int8_t t = p.cell_type[i];
+            if (t == kLiquid && p.layer_id[i] == 0)
+                liquid++;
+            if ((t == kLiquid || t == kActive) && p.du[i] == 0.0f)
+                zero_du = 1;
+        }
     }
     d.liquid = liquid;
     d.zero_du = zero_du;
@@ -1917,7 +2002,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
         int nseeds = (int)(p.voronoi_seeds.size() / 3);
         int32_t *dseeds = nullptr;
         if (nseeds) {
-            CUDA_OK(cudaMalloc(&dseeds, p.voronoi_seeds.size() * 4));
+            CUDA_OK(cudaMallocAsync((void **)&dseeds, p.voronoi_seeds.size() * 4, st));
             CUDA_OK(cudaMemcpyAsync(dseeds, p.voronoi_seeds.data(), p.voronoi_seeds.size() * 4,
                                     cudaMemcpyHostToDevice, st));
         }
@@ -1925,10 +2010,8 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
         k_voronoi<<<(unsigned)blocks, 256, 3 * 1024 * sizeof(int), st>>>(ddesc_ + slot, dseeds, nseeds,
                                                                          (float)(g.active_size));
         CUDA_OK(cudaGetLastError());
-        if (dseeds) {
-            CUDA_OK(cudaStreamSynchronize(st));
-            CUDA_OK(cudaFree(dseeds));
-        }
+        if (dseeds)
+            CUDA_OK(cudaFreeAsync(dseeds, st));
     }
     // register the domain, then build its initial active list in the list the next cycle consumes
     n_domains_ = std::max(n_domains_, slot + 1);
@@ -1952,17 +2035,17 @@ void Pool::retire(int slot) {
                             cudaMemcpyHostToDevice, st));
     k_drop_domain<<<num_sms_ * 2, 256, 0, st>>>(dstate_, (unsigned)slot, (unsigned)max_domains_);
     CUDA_OK(cudaGetLastError());
-    CUDA_OK(cudaStreamSynchronize(st));
     DomainDesc zero;
     std::memset(&zero, 0, sizeof(zero));
     zero.done = 1;
     host_desc_[slot] = zero;
+    // the copies from host memory are staged before each call returns; everything below runs in
+    // stream order after the cycles already queued, so nothing waits here
     CUDA_OK(cudaMemcpyAsync(ddesc_ + slot, &zero, sizeof(zero), cudaMemcpyHostToDevice, st));
-    CUDA_OK(cudaStreamSynchronize(st));
     for (void *p : s.allocs)
-        CUDA_OK(cudaFree(p));
+        CUDA_OK(cudaFreeAsync(p, st));
     if (s.growth)
-        CUDA_OK(cudaFree(s.growth));
+        CUDA_OK(cudaFreeAsync(s.growth, st));
     bytes_in_use_ -= s.bytes;
     s = SlotHost();
 }
@@ -2074,6 +2157,8 @@ PoolStats Pool::stats() {
     std::memset(&r, 0, sizeof(r));
     r.cycles = cycles_launched_;
     r.launches = launches_;
+    r.h2d_bytes = h2d_bytes_;
+    r.d2h_bytes = d2h_bytes_;
     for (int q = 0; q < kStatShards; q++) {
         r.listed += ps.stat[q][kStatListed];
         r.grown += ps.stat[q][kStatGrown];
@@ -2355,6 +2440,7 @@ void Pool::copy_out_raw(int slot, int32_t *grain_id, int8_t *cell_type) {
     cudaStream_t st = S(stream_);
     if (grain_id)
         CUDA_OK(cudaMemcpyAsync(grain_id, d.gid, N * 4, cudaMemcpyDeviceToHost, st));
+    d2h_bytes_ += (grain_id ? N * 4 : 0) + (cell_type ? N : 0);
     if (cell_type)
         CUDA_OK(cudaMemcpyAsync(cell_type, d.ctype, N, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
@@ -2375,6 +2461,7 @@ void Pool::copy_octahedra(int slot, float *dl, float *doc, float *cdl) {
     cudaStream_t st = S(stream_);
     if (dl)
         CUDA_OK(cudaMemcpyAsync(dl, d.dl + o, A * 4, cudaMemcpyDeviceToHost, st));
+    d2h_bytes_ += (dl ? A * 4 : 0) + (doc ? A * 12 : 0) + (cdl ? A * 104 : 0);
     if (doc)
         CUDA_OK(cudaMemcpyAsync(doc, d.doc + 3 * o, A * 12, cudaMemcpyDeviceToHost, st));
     if (cdl)
@@ -2579,6 +2666,7 @@ GrainStats Pool::grain_stats(int slot, const int *region) {
     if (!slot_used(slot))
         throw std::invalid_argument("bad slot");
     const Problem &p = *slots_[slot].problem;
+    materialize_fields(p);
     const Geometry &g = p.g;
     Region R;
     if (region) {

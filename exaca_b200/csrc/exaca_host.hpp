@@ -6,6 +6,8 @@
 #pragma once
 
 #include <cstdint>
+#include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -87,17 +89,29 @@ struct Geometry {
     int procs_x = 1, procs_y = 1;
 };
 
+// What the per-cell fields of a type-C problem are made of: they are written on the device at
+// admission (src/CAinitialize.cpp:1025-1055, 1460-1529, 1834-2206 as one pass over the cells plus
+// the scatter of the seeds and nuclei), and on the host only when a caller asks for them.
+struct DirectionalSeeds {
+    bool used = false;
+    std::vector<int32_t> plane_cts; // CritTimeStep of each z plane
+    std::vector<int64_t> active;    // substrate seeds (initially active cells), ascending; GrainID rank + 1
+};
+
 // A fully initialised problem, ready to be admitted to a device pool.
 struct Problem {
     InputConfig cfg;
     Geometry g;
-    // per-cell fields over the whole domain (index k*mx*my + i*my + j, y fastest)
-    std::vector<int32_t> cts;      // CritTimeStep
-    std::vector<int8_t> layer_id;  // LayerID (single layer: -1 or 0)
-    std::vector<float> du;         // UndercoolingChange
-    std::vector<int8_t> cell_type; // CellType
-    std::vector<int32_t> grain_id; // GrainID
-    std::vector<uint8_t> melted;   // Melted
+    // per-cell fields over the whole domain (index k*mx*my + i*my + j, y fastest); for a type-C
+    // problem (dir.used) empty until materialize_fields fills them
+    mutable std::vector<int32_t> cts;      // CritTimeStep
+    mutable std::vector<int8_t> layer_id;  // LayerID (single layer: -1 or 0)
+    mutable std::vector<float> du;         // UndercoolingChange
+    mutable std::vector<int8_t> cell_type; // CellType
+    mutable std::vector<int32_t> grain_id; // GrainID
+    mutable std::vector<uint8_t> melted;   // Melted
+    DirectionalSeeds dir;
+    std::shared_ptr<std::mutex> fields_mutex = std::make_shared<std::mutex>();
     // orientation table: 9 floats per orientation (src/CAinitialize.cpp:1408-1441)
     std::vector<float> guv;
     // fresh-octahedron critical diagonal lengths, 26 per orientation
@@ -135,6 +149,10 @@ std::string find_data_file(const std::string &name, const std::string &type, std
 // Builds the geometry, temperature field, substrate, grains and nuclei of a C or S problem
 // (src/CAinitialize.cpp:579-2769). Throws for unsupported problem kinds.
 void initialize_problem(Problem &p, std::string &log);
+
+// Fills the per-cell host fields of a problem whose fields are made on the device (type C); a
+// no-op when they are already there. Safe to call from several threads.
+void materialize_fields(const Problem &p);
 
 // Page-locks the per-cell host vectors (cudaHostRegister) for fast admission copies.
 void pin_problem(Problem &p);

@@ -764,7 +764,96 @@ void nuclei_init(Problem &p, std::string &log) {
     log += "(0: " + std::to_string(p.nuclei_loc.size()) + ") ";
 }
 
+// Type C without the per-cell host fields (src/CAinitialize.cpp:1025-1055, 1460-1529, 1834-2247):
+// the plane CritTimeSteps, the substrate seeds and the nuclei come from the same random streams
+// in the same orders as the dense path above; the dense fields are made from them on the device at
+// admission (and by materialize_fields on the host).
+void init_directional_seeds(Problem &p, std::string &log) {
+    Geometry &g = p.g;
+    const InputConfig &c = p.cfg;
+    g.zbound_low = 0;
+    g.zbound_high = g.nz - 1;
+    g.nz_active = g.nz;
+    DirectionalSeeds &d = p.dir;
+    d.used = true;
+    d.plane_cts.resize(g.nz);
+    for (int k = 0; k < g.nz; k++)
+        d.plane_cts[k] = (int)(((k - 1) * c.G * c.deltax) / (c.R * c.deltat));
+    p.du_value = c.R * c.deltat;
+    // substrate: one draw per cell of plane k = 1 inside the ghost ring, in (i, j) order
+    {
+        std::mt19937_64 gen(0);
+        std::uniform_real_distribution<double> dis(0.0, 1.0);
+        d.active.clear();
+        for (int i = 1; i < g.mx - 1; i++)
+            for (int j = 1; j < g.my - 1; j++)
+                if (dis(gen) < c.fract_surface_sites_active)
+                    d.active.push_back(cell_index(g, 1, i, j));
+    }
+    // potential nuclei: one draw per cell with CritTimeStep != 0, planes k = 1 .. nz-2 in (k, j, i)
+    // order; numbered -1, -2, ... in index order
+    std::vector<int32_t> sites;
+    {
+        std::mt19937_64 gen(0);
+        std::uniform_real_distribution<double> dis(0.0, 1.0);
+        const double bulk_prob = c.nmax * c.deltax * c.deltax * c.deltax;
+        for (int k = 1; k < g.nz - 1; k++) {
+            if (d.plane_cts[k] == 0)
+                continue;
+            for (int j = 1; j < g.my - 1; j++)
+                for (int i = 1; i < g.mx - 1; i++)
+                    if (dis(gen) < bulk_prob)
+                        sites.push_back((int32_t)cell_index(g, k, i, j));
+        }
+    }
+    std::sort(sites.begin(), sites.end());
+    {
+        std::default_random_engine generator;
+        std::normal_distribution<double> distribution(c.dTN, c.dTsigma);
+        p.nuclei_loc = sites;
+        p.nuclei_time.resize(sites.size());
+        for (size_t n = 0; n < sites.size(); n++) {
+            const int cts = d.plane_cts[sites[n] / (g.mx * g.my)];
+            const double und = distribution(generator);
+            const int t = cts + round(und / p.du_value);
+            p.nuclei_time[n] = std::max(cts, t);
+        }
+    }
+    p.possible_nuclei = (int)sites.size();
+}
+
 } // namespace
+
+void materialize_fields(const Problem &p) {
+    if (!p.dir.used)
+        return;
+    std::lock_guard<std::mutex> lock(*p.fields_mutex);
+    if (!p.cell_type.empty())
+        return;
+    const Geometry &g = p.g;
+    const long N = g.domain_size;
+    p.cts.resize(N);
+    p.layer_id.assign(N, 0);
+    p.du.assign(N, p.du_value);
+    p.cell_type.resize(N);
+    p.grain_id.assign(N, 0);
+    p.melted.resize(N);
+    for (int k = 0; k < g.nz; k++)
+        for (int i = 0; i < g.mx; i++)
+            for (int j = 0; j < g.my; j++) {
+                const long idx = cell_index(g, k, i, j);
+                const bool wall = i == 0 || i == g.mx - 1 || j == 0 || j == g.my - 1 || k == 0 || k == g.nz - 1;
+                p.cts[idx] = p.dir.plane_cts[k];
+                p.cell_type[idx] = wall ? kWall : kLiquid;
+                p.melted[idx] = wall ? 0 : 1;
+            }
+    for (size_t n = 0; n < p.dir.active.size(); n++) {
+        p.cell_type[p.dir.active[n]] = kActive;
+        p.grain_id[p.dir.active[n]] = (int32_t)(n + 1);
+    }
+    for (size_t n = 0; n < p.nuclei_loc.size(); n++)
+        p.grain_id[p.nuclei_loc[n]] = -(int32_t)(n + 1);
+}
 
 void initialize_problem(Problem &p, std::string &log) {
     auto t0 = std::chrono::steady_clock::now();
@@ -794,6 +883,31 @@ void initialize_problem(Problem &p, std::string &log) {
     if ((long)g.mx * g.my * g.nz > 2000000000L)
         throw Unsupported("domain too large: the cell index must fit in 31 bits");
 
+    // Type C with more than one interior cell (then no liquid cell is cut off by walls) keeps no
+    // per-cell host fields: they are made on the device
+    const bool seeds_only = c.simulation_type == "C" && (g.nx > 3 || g.ny > 3 || g.nz > 3);
+    if (seeds_only) {
+        init_directional_seeds(p, log);
+        g.active_size = (long)g.mx * g.my * g.nz_active;
+        log += "Done with temperature field initialization, active domain size is " + std::to_string(g.nz_active) +
+               " out of " + std::to_string(g.nz) + " cells in the Z direction\n";
+        read_orientations(c.orientation_file, p.guv);
+        build_cdl_table(p.guv, p.cdl_table);
+        log += "Done with orientation initialization \n";
+        log += "Number of potential nucleated grains: " + std::to_string(p.nuclei_loc.size()) + "\n";
+        log += "Grain struct initialized\n";
+        log += " Possible nucleation events (rank: # events): \n";
+        log += "(0: " + std::to_string(p.nuclei_loc.size()) + ") ";
+        log += "Nucleation initialized\n";
+        p.A_n = c.A * c.deltat / c.deltax;
+        p.B_n = c.B * c.deltat / c.deltax;
+        p.C_n = c.C * c.deltat / c.deltax;
+        p.D_n = c.D;
+        p.du_values.clear();
+        p.du_class.clear();
+        p.init_seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        return;
+    }
     p.cts.assign(g.domain_size, 0);
     p.layer_id.assign(g.domain_size, 0);
     p.du.assign(g.domain_size, 0.0f);

@@ -204,6 +204,7 @@ void write_vtk_fields(const Problem &p, const int32_t *grain_id, const std::stri
     // src/CAprint.cpp:285-346 with PrintFullOutput: LayerID, GrainID, Melted
     if (threads <= 0)
         threads = output_threads();
+    materialize_fields(p);
     File o(fname);
     const Geometry &g = p.g;
     vtk_header(o, g.nx, g.ny, g.nz);
@@ -215,6 +216,7 @@ void write_vtk_fields(const Problem &p, const int32_t *grain_id, const std::stri
 void write_debug_vtk(const Problem &p, const std::string &fname) {
     // src/CAprint.cpp:285-395 with PrintFullOutput false: the init debug dump of PrintDebug 1 or 2
     const int threads = output_threads();
+    materialize_fields(p);
     File o(fname);
     const Geometry &g = p.g;
     vtk_header(o, g.nx, g.ny, g.nz);
@@ -237,6 +239,7 @@ void write_misorientations(const Problem &p, const int32_t *grain_id, const std:
     // src/CAprint.cpp:398-460
     if (threads <= 0)
         threads = output_threads();
+    materialize_fields(p);
     const Geometry &g = p.g;
     File o(fname);
     o.put("# vtk DataFile Version 3.0\nvtk output\nASCII\nDATASET STRUCTURED_POINTS\n");

@@ -152,6 +152,8 @@ struct PoolStats {
     unsigned long long cycles; // CA cycles launched
     unsigned long long launches; // kernels launched by step()
     unsigned long long listed, grown, captured, nucleated, claims, row_reads, dropped, fresh, rechecks, flagged;
+    unsigned long long h2d_bytes, d2h_bytes; // problem data copied host->device (fields or seeds, nuclei,
+                                             // tables) and results copied back
 };
 
 // CUDA-event times of a stretch of cycles run pass by pass as separate kernels.
@@ -289,6 +291,7 @@ class Pool {
     int graph_steps_ = 0;
     int grid_claim_ = 0;
     unsigned long long launches_ = 0;
+    unsigned long long h2d_bytes_ = 0, d2h_bytes_ = 0;
     double last_run_ms_ = 0;
     void *census_buf_ = nullptr;
 };

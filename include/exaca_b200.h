@@ -21,7 +21,7 @@ extern "C" {
 
 #define EXACA_OK 0
 #define EXACA_ERR_INPUT (-1)     /* malformed input file, missing key or data file */
-#define EXACA_ERR_UNSUPPORTED (-2) /* a problem kind this solver does not handle (type R, >1 layer) */
+#define EXACA_ERR_UNSUPPORTED (-2) /* a problem this solver does not handle (substrate file, >127 layers, ...) */
 #define EXACA_ERR_CUDA (-3)      /* CUDA runtime failure or device-side error flag */
 #define EXACA_ERR_BUDGET (-4)    /* admission refused: HBM budget or slot limit */
 #define EXACA_ERR_ARG (-5)       /* bad handle, slot or size */
@@ -81,6 +81,9 @@ typedef struct {
     uint64_t fresh;     /* liquid-neighbour masks built from the 26 neighbour types */
     uint64_t rechecks;  /* solidification re-checks next to claimed cells */
     uint64_t flagged;   /* records handed from the growth pass to the claim pass */
+    uint64_t h2d_bytes; /* problem data copied host->device: cell fields (or, for type C, the seeds
+                           they are made from on the device), nuclei, growth and orientation tables */
+    uint64_t d2h_bytes; /* results copied device->host (GrainID, CellType, octahedron state) */
 } exaca_pool_stats_t;
 
 /* The reference's every-1000-cycle census (src/CAupdate.cpp:738-808). */
