@@ -122,6 +122,7 @@ SIGNATURES = {
     "exaca_pool_stats": ([_P, ctypes.POINTER(PoolStatsT)], _I),
     "exaca_pool_run_plain": ([_P, _I, _I, ctypes.POINTER(_I)], _I),
     "exaca_pool_copy_out": ([_P, _I, _P, _P], _I),
+    "exaca_pool_copy_out_concurrent": ([_P, _I, _P, _P], _I),
     "exaca_pool_copy_octahedra": ([_P, _I, _P, _P, _P], _I),
     "exaca_pool_retire": ([_P, _I], _I),
     "exaca_pool_bytes_in_use": ([_P], ctypes.c_int64),
@@ -326,6 +327,15 @@ class Pool:
         gid = np.empty(n, np.int32)
         ct = np.empty(n, np.int32)
         _check(load_library().exaca_pool_copy_out(self._h, slot, _ptr(gid), _ptr(ct)))
+        return gid, ct
+
+    def copy_out_concurrent(self, slot: int):
+        """copy_out of a slot whose domain has ended (per the last status): does not wait for cycles
+        launched since, so finished results can be fetched while the next cycles run."""
+        n = self._problems[slot].geometry.domain_size
+        gid = np.empty(n, np.int32)
+        ct = np.empty(n, np.int32)
+        _check(load_library().exaca_pool_copy_out_concurrent(self._h, slot, _ptr(gid), _ptr(ct)))
         return gid, ct
 
     def copy_octahedra(self, slot: int):

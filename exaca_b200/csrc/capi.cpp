@@ -426,6 +426,12 @@ int exaca_pool_copy_out(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *
     });
 }
 
+int exaca_pool_copy_out_concurrent(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *cell_type) {
+    if (!pool || !pool->pool->slot_used(slot))
+        return fail(EXACA_ERR_ARG, "bad slot");
+    return guarded([&] { pool->pool->copy_out_concurrent(slot, grain_id, cell_type); });
+}
+
 int exaca_pool_copy_octahedra(exaca_pool *pool, int slot, float *dl, float *doc, float *cdl) {
     if (!pool || !pool->pool->slot_used(slot))
         return fail(EXACA_ERR_ARG, "bad slot");

@@ -1762,6 +1762,8 @@ Pool::~Pool() {
     cudaFree(ddesc_);
     cudaFree(census_buf_);
     cudaStreamDestroy(S(stream_));
+    if (copy_stream_)
+        cudaStreamDestroy(S(copy_stream_));
 }
 
 const DeviceTables &Pool::tables_for(const Problem &p) {
@@ -2475,6 +2477,36 @@ void Pool::copy_out(int slot, int32_t *grain_id, int32_t *cell_type) {
     if (cell_type)
         ct.resize(N);
     copy_out_raw(slot, grain_id, cell_type ? ct.data() : nullptr);
+    if (cell_type)
+        for (size_t i = 0; i < N; i++)
+            cell_type[i] = ct[i];
+}
+
+void Pool::copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type) {
+    CUDA_OK(cudaSetDevice(device_));
+    const SlotHost &s = slots_.at(slot);
+    const DomainDesc &d = host_desc_.at(slot);
+    if (!s.used || !(d.done || s.finished))
+        throw std::invalid_argument("copy_out_concurrent: the slot's domain has not ended");
+    if (!copy_stream_) {
+        cudaStream_t cs;
+        CUDA_OK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+        copy_stream_ = cs;
+    }
+    // The domain's GrainID and CellType are final (an ended domain's records only leave the list),
+    // and the host saw that state, so the copies need no ordering against the pool stream. Copy
+    // engines only: no kernel runs beside the persistent cooperative one.
+    cudaStream_t cs = S(copy_stream_);
+    const size_t N = s.problem->g.domain_size;
+    std::vector<int8_t> ct;
+    if (grain_id)
+        CUDA_OK(cudaMemcpyAsync(grain_id, d.gid, N * 4, cudaMemcpyDeviceToHost, cs));
+    if (cell_type) {
+        ct.resize(N);
+        CUDA_OK(cudaMemcpyAsync(ct.data(), d.ctype, N, cudaMemcpyDeviceToHost, cs));
+    }
+    CUDA_OK(cudaStreamSynchronize(cs));
+    d2h_bytes_ += (grain_id ? N * 4 : 0) + (cell_type ? N : 0);
     if (cell_type)
         for (size_t i = 0; i < N; i++)
             cell_type[i] = ct[i];

@@ -214,6 +214,10 @@ class Pool {
     Census census(int slot);
     void copy_out(int slot, int32_t *grain_id, int32_t *cell_type);
     void copy_out_raw(int slot, int32_t *grain_id, int8_t *cell_type);
+    // copy_out of a slot whose domain has ended (as of the last state read) on a separate copy
+    // stream: it does not wait for cycles launched since, so a request loop can copy finished
+    // results while the next cycles run. Returns when the data is on the host.
+    void copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type);
     void copy_octahedra(int slot, float *dl, float *doc, float *cdl);
     // writes the diagonal lengths held in the active records back to the per-cell array
     void flush_records();
@@ -269,7 +273,8 @@ class Pool {
     int device_;
     size_t budget_;
     size_t bytes_in_use_ = 0;
-    void *stream_ = nullptr; // cudaStream_t
+    void *stream_ = nullptr;      // cudaStream_t
+    void *copy_stream_ = nullptr; // cudaStream_t of copy_out_concurrent (created on first use)
     PoolState *dstate_ = nullptr;
     DomainDesc *ddesc_ = nullptr;
     int max_domains_ = 0;

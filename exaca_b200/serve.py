@@ -3,8 +3,11 @@
 Requests (directional-solidification solves) arrive as a Poisson stream. Each is initialised on a
 host worker as soon as it arrives, admitted into the device pool as soon as it is initialised and
 its HBM footprint fits the budget, stepped together with every other resident domain, and retired
-(result copied out, memory freed) when it has met the reference's termination test. A domain's
-result does not depend on the others in the pool, so each result equals its own plain run.
+(result copied out, memory freed) when it has met the reference's termination test. The results
+of the domains that ended in one stretch of cycles are copied out while the next stretch runs (a
+separate copy stream), and admission and retirement queue behind running cycles, so the device
+steps while the host does its part. A domain's result does not depend on the others in the pool,
+so each result equals its own plain run.
 """
 from __future__ import annotations
 
@@ -58,6 +61,7 @@ def serve(requests: list, device: int = 0, budget_bytes: int = 150 * 10**9, chun
     results = [None] * n
     waiting = []  # initialised, not admitted yet (arrival order)
     resident = {}  # slot -> request index
+    finished = []  # (slot, request index, final cycle) ended at the last status read
     done_count = 0
     steps = 0
     try:
@@ -85,23 +89,28 @@ def serve(requests: list, device: int = 0, budget_bytes: int = 150 * 10**9, chun
                             raise
                 still.append((k, prob))
             waiting = still
-            if not resident:
+            if not resident and not finished:
                 time.sleep(0.0005)
                 continue
-            pool.step(chunk_cycles)
-            steps += 1
-            slots = list(resident)
-            for slot, st in zip(slots, pool.status_many(slots)):
-                if st.error:
-                    raise ExacaError(-3, f"device error flags {st.error} in slot {slot}")
-                if st.done:
-                    k = resident.pop(slot)
-                    g, c = pool.copy_out(slot)
-                    pool.retire(slot)
-                    latency[k] = time.perf_counter() - t_start - requests[k][0]
-                    if keep_results:
-                        results[k] = (g, c, st.cycle)
-                    done_count += 1
+            if resident:
+                pool.step(chunk_cycles)  # returns at launch
+                steps += 1
+            # results of the domains that ended before this stretch, while it runs
+            for slot, k, cycle in finished:
+                g, c = pool.copy_out_concurrent(slot)
+                pool.retire(slot)
+                latency[k] = time.perf_counter() - t_start - requests[k][0]
+                if keep_results:
+                    results[k] = (g, c, cycle)
+                done_count += 1
+            finished = []
+            if resident:
+                slots = list(resident)
+                for slot, st in zip(slots, pool.status_many(slots)):
+                    if st.error:
+                        raise ExacaError(-3, f"device error flags {st.error} in slot {slot}")
+                    if st.done:
+                        finished.append((slot, resident.pop(slot), st.cycle))
         elapsed = time.perf_counter() - t_start
     finally:
         workers.shutdown(wait=True)

@@ -167,6 +167,12 @@ double exaca_pool_last_run_ms(exaca_pool *pool);
 int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms);
 /* Device->host copy of GrainID and CellType (src/runCA.cpp:423-424); NULL skips a field. */
 int exaca_pool_copy_out(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *cell_type);
+/* exaca_pool_copy_out for a slot whose domain has ended as of the last exaca_pool_status(_many) /
+ * run_plain: the copies use the pool's separate copy stream and do not wait for cycles launched
+ * since, so a request loop can fetch finished results while the next cycles run (the reference's
+ * copy-back, src/runCA.cpp:423-424, once per finished request). Returns when the data is on the
+ * host; EXACA_ERR_ARG if the domain has not ended. */
+int exaca_pool_copy_out_concurrent(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *cell_type);
 /* Active-window octahedron state (DiagonalLength, DOCenter x3, CritDiagonalLength x26) of the
  * slot's current layer: window_nz * mx * my cells from plane window_z_lo (exaca_pool_status), the
  * reference's window arrays (src/runCA.cpp:147-151, resized per layer at :352-356). */
