@@ -1488,6 +1488,11 @@ __global__ void k_fill_directional(int8_t *ctype, int32_t *gid, int32_t *cts, in
     }
 }
 
+__global__ void k_widen_types(const int8_t *ctype, int32_t *out, long long n) {
+    for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (long long)gridDim.x * blockDim.x)
+        out[c] = ctype[c];
+}
+
 __global__ void k_scatter_seeds(int8_t *ctype, int32_t *gid, const long long *active, long long n_active,
                                 const int32_t *nuclei, long long n_nuclei) {
     const long long q = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -2472,14 +2477,27 @@ void Pool::copy_octahedra(int slot, float *dl, float *doc, float *cdl) {
 }
 
 void Pool::copy_out(int slot, int32_t *grain_id, int32_t *cell_type) {
-    size_t N = slots_.at(slot).problem->g.domain_size;
-    std::vector<int8_t> ct;
-    if (cell_type)
-        ct.resize(N);
-    copy_out_raw(slot, grain_id, cell_type ? ct.data() : nullptr);
-    if (cell_type)
-        for (size_t i = 0; i < N; i++)
-            cell_type[i] = ct[i];
+    if (!cell_type) {
+        copy_out_raw(slot, grain_id, nullptr);
+        return;
+    }
+    // CellType is widened to int32 on the device (in stream order after the cycles), so both fields
+    // go straight into the caller's buffers (a DMA when they are pinned) with no host pass
+    CUDA_OK(cudaSetDevice(device_));
+    const DomainDesc &d = host_desc_.at(slot);
+    const size_t N = slots_.at(slot).problem->g.domain_size;
+    cudaStream_t st = S(stream_);
+    int32_t *wide = nullptr;
+    CUDA_OK(cudaMallocAsync((void **)&wide, std::max<size_t>(N * 4, 16), st));
+    const unsigned blocks = (unsigned)std::min<size_t>((N + 255) / 256, (size_t)num_sms_ * 16);
+    k_widen_types<<<blocks, 256, 0, st>>>(d.ctype, wide, (long long)N);
+    CUDA_OK(cudaGetLastError());
+    if (grain_id)
+        CUDA_OK(cudaMemcpyAsync(grain_id, d.gid, N * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaMemcpyAsync(cell_type, wide, N * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_OK(cudaFreeAsync(wide, st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    d2h_bytes_ += (grain_id ? N * 4 : 0) + N * 4;
 }
 
 void Pool::copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type) {
