@@ -6,6 +6,8 @@
 // GrainID / CellType arrays, final cycle and post-init fields of the reference itself (compiled
 // from its unmodified sources against single-rank shims), stored in tests/golden/*.npz.
 //
+// Problem types C, S and R (temperature files), one or several layers; no substrate files.
+//
 // The restatement follows the reference's loops literally, in its serial (Kokkos-Serial) order:
 // every function cites the reference lines it follows (paths relative to the reference project).
 // The arithmetic is the reference's: same types, same operation order, libm pow/sqrt/sqrtf, the
@@ -42,7 +44,7 @@ const int NGrainOrientations = 10000;
 
 thread_local std::string g_error;
 
-// ---- input file (src/CAinitialize.cpp:24-576, the C and S branches) --------------------------
+// ---- input file (src/CAinitialize.cpp:24-576) ---------------------------------------------------
 struct Input {
     std::string type;
     double A, B, C, D, freezing;
@@ -50,6 +52,10 @@ struct Input {
     int nx, ny, nz, nspx, nspy, spot_offset, spot_radius, layers, layer_height;
     float grain_spacing;
     std::string orientation_file;
+    // type R
+    double ht_deltax = 0;
+    std::vector<std::string> temp_paths;
+    bool extra_walls = false;
 };
 
 struct Reader {
@@ -62,8 +68,10 @@ struct Reader {
             if (l == "*****")
                 break;
     }
-    // key check by substring; the value is everything after the colon, whitespace removed
-    std::string value(const std::string &key) {
+    std::string last_key; // the key of the last value read
+    // key check by substring (key, or alt when given); the value is everything after the colon,
+    // whitespace removed
+    std::string value(const std::string &key, const std::string &alt = "") {
         std::string line;
         for (;;) {
             if (!std::getline(in, line))
@@ -76,8 +84,9 @@ struct Reader {
                               k.find("Source of input length unit") != std::string::npos;
             if (deprecated)
                 continue;
-            if (k.find(key) == std::string::npos)
+            if (k.find(key) == std::string::npos && (alt.empty() || k.find(alt) == std::string::npos))
                 throw std::runtime_error("expected key " + key);
+            last_key = k;
             std::string v;
             for (char ch : line.substr(c + 1))
                 if (!std::isspace((unsigned char)ch))
@@ -137,10 +146,229 @@ Input read_input(const std::string &path, const std::string &data_dir) {
         I.nx = 4 + 2 * I.spot_radius + I.spot_offset * (I.nspx - 1);
         I.ny = 4 + 2 * I.spot_radius + I.spot_offset * (I.nspy - 1);
     }
+    else if (I.type == "R") {
+        // src/CAinitialize.cpp:321-392
+        I.ht_deltax = atof(r.value("Heat transport data mesh size").c_str()) * pow(10, -6);
+        I.deltat = atof(r.value("Time step").c_str()) * pow(10, -6);
+        std::string v = r.value("Path to substrate file", "Substrate grain spacing");
+        if (r.last_key.find("Substrate grain spacing") == std::string::npos)
+            throw std::runtime_error("oracle: substrate files are not restated");
+        I.grain_spacing = atof(v.c_str());
+        std::string path = r.value("Path to temperature file"), name = r.value("Temperature filename");
+        int nfiles = std::stoi(r.value("Number of temperature files"));
+        for (int i = 1; i <= nfiles; i++)
+            I.temp_paths.push_back(path + "/" + (nfiles > 1 ? std::to_string(i) + name : name));
+        I.extra_walls = r.value("Extra set of wall cells") == "Y";
+        I.layers = std::stoi(r.value("Number of layers"));
+        I.layer_height = std::stoi(r.value("Offset between layers"));
+    }
     else {
-        throw std::runtime_error("oracle: problem types C and S only");
+        throw std::runtime_error("oracle: problem types C, S and R only");
     }
     return I;
+}
+
+// ---- type R temperature data (src/CAinitialize.cpp:135-198, 747-1003, 1128-1405) ------------------
+// split at commas: the first n-1 fields, then the rest of the line (src/CAinitialize.cpp:135-146)
+std::vector<double> temperature_values(std::string line, int n) {
+    std::vector<double> out(n);
+    for (int q = 0; q < n - 1; q++) {
+        std::size_t pos = line.find(',');
+        out[q] = std::stod(line.substr(0, pos));
+        line = line.substr(pos + 1);
+    }
+    out[n - 1] = std::stod(line);
+    return out;
+}
+
+struct TemperatureGrid {
+    std::vector<double> raw; // 6 values per stored point (RawData)
+    std::vector<int> first, last;
+    std::vector<float> zmin_layer, zmax_layer;
+    float XMin, XMax, YMin, YMax, ZMin, ZMax;
+    std::vector<int> finish;
+};
+
+// ParallelMeshInit's type-R branch at one rank (src/CAinitialize.cpp:747-1003): bounds from every
+// file, domain sizes, then the points of x/y range [2, nx-3] x [2, ny-3] (the one rank's range)
+void mesh_reduced(Input &I, TemperatureGrid &T) {
+    T.XMin = 1000000.0;
+    T.YMin = 1000000.0;
+    T.ZMin = 1000000.0;
+    T.XMax = -1000000.0;
+    T.YMax = -1000000.0;
+    T.ZMax = -1000000.0;
+    const int nfiles = (int)I.temp_paths.size(), L = I.layers;
+    T.zmin_layer.assign(L, 0.0f);
+    T.zmax_layer.assign(L, 0.0f);
+    T.first.assign(L, 0);
+    T.last.assign(L, 0);
+    const int read = std::min(L, nfiles);
+    for (int f = 1; f <= read; f++) {
+        std::ifstream in(I.temp_paths[f - 1]);
+        std::string line;
+        std::getline(in, line);
+        if (line.find("Number of temperature data points") != std::string::npos)
+            throw std::runtime_error("oracle: old temperature format");
+        double x0 = 1e300, x1 = -1e300, y0 = 1e300, y1 = -1e300, z0 = 1e300, z1 = -1e300;
+        while (std::getline(in, line) && !line.empty()) {
+            std::vector<double> v = temperature_values(line, 3);
+            x0 = std::min(x0, v[0]);
+            x1 = std::max(x1, v[0]);
+            y0 = std::min(y0, v[1]);
+            y1 = std::max(y1, v[1]);
+            z0 = std::min(z0, v[2]);
+            z1 = std::max(z1, v[2]);
+        }
+        z0 += I.deltax * I.layer_height * (f - 1);
+        z1 += I.deltax * I.layer_height * (f - 1);
+        if (x0 < T.XMin)
+            T.XMin = x0;
+        if (x1 > T.XMax)
+            T.XMax = x1;
+        if (y0 < T.YMin)
+            T.YMin = y0;
+        if (y1 > T.YMax)
+            T.YMax = y1;
+        if (z0 < T.ZMin)
+            T.ZMin = z0;
+        if (z1 > T.ZMax)
+            T.ZMax = z1;
+        T.zmin_layer[f - 1] = z0;
+        T.zmax_layer[f - 1] = z1;
+    }
+    for (int f = nfiles; f < L; f++) {
+        if (nfiles == 1) {
+            T.zmin_layer[f] = T.zmin_layer[f - 1] + I.deltax * I.layer_height;
+            T.zmax_layer[f] = T.zmax_layer[f - 1] + I.deltax * I.layer_height;
+        }
+        else {
+            int rep = f % nfiles, unit = f / nfiles;
+            T.zmin_layer[f] = T.zmin_layer[rep] + unit * nfiles * I.deltax * I.layer_height;
+            T.zmax_layer[f] = T.zmax_layer[rep] + unit * nfiles * I.deltax * I.layer_height;
+        }
+        T.ZMax += I.deltax * I.layer_height;
+    }
+    I.nx = round((T.XMax - T.XMin) / I.deltax) + 1 + 4;
+    I.ny = round((T.YMax - T.YMin) / I.deltax) + 1 + 4;
+    I.nz = round((T.ZMax - T.ZMin) / I.deltax) + 1 + 3;
+    for (int f = 1; f <= read; f++) {
+        std::ifstream in(I.temp_paths[f - 1]);
+        std::string line;
+        std::getline(in, line);
+        T.first[f - 1] = (int)T.raw.size();
+        while (std::getline(in, line) && !line.empty()) {
+            std::vector<double> v = temperature_values(line, 6);
+            int xi = round((v[0] - T.XMin) / I.deltax) + 2, yi = round((v[1] - T.YMin) / I.deltax) + 2;
+            if (xi >= 2 && xi <= I.nx - 3 && yi >= 2 && yi <= I.ny - 3)
+                T.raw.insert(T.raw.end(), v.begin(), v.end());
+        }
+        T.last[f - 1] = (int)T.raw.size();
+    }
+    for (int f = nfiles; f < L; f++) {
+        int from = nfiles == 1 ? f - 1 : f % nfiles;
+        T.first[f] = T.first[from];
+        T.last[f] = T.last[from];
+    }
+}
+
+// TempInit_Reduced at one rank (src/CAinitialize.cpp:1128-1405)
+void temp_reduced(Input &I, TemperatureGrid &T, int MX, int MY, int nz, std::vector<int> &CTS, std::vector<float> &DU,
+                  std::vector<int> &Layer, int &ZBound_High, int &nzActive) {
+    double unrounded = I.ht_deltax / I.deltax, fl = floor(unrounded);
+    if (unrounded - fl > 0.0005)
+        throw std::runtime_error("oracle: temperature spacing not a multiple of the cell size");
+    I.deltax = I.ht_deltax / fl;
+    const int ratio = round(I.ht_deltax / I.deltax);
+    const int lx = 2, ly = 2, ux = I.nx - 3, uy = I.ny - 3; // one rank: MyXOffset = MyYOffset = -1
+    const int sx = ux - lx + 1, sy = uy - ly + 1;
+    for (long p = 0; p < (long)MX * MY * nz; p++)
+        Layer[p] = -1;
+    T.finish.assign(I.layers, 0);
+    for (int L = 0; L < I.layers; L++) {
+        double small = 1000000000, large = 0;
+        int nzt = round((T.zmax_layer[L] - T.zmin_layer[L]) / I.deltax) + 1;
+        std::vector<std::vector<std::vector<double>>> CR(nzt, std::vector<std::vector<double>>(sx, std::vector<double>(sy, -1.0)));
+        std::vector<std::vector<std::vector<double>>> TL = CR;
+        int X = -1, Y = -1, Z = -1;
+        for (int i = T.first[L]; i < T.last[L]; i++) {
+            int pos = i % 6;
+            if (pos == 0)
+                X = round((T.raw[i] - T.XMin) / I.deltax) + 2;
+            else if (pos == 1)
+                Y = round((T.raw[i] - T.YMin) / I.deltax) + 2;
+            else if (pos == 2)
+                Z = round((T.raw[i] + I.deltax * I.layer_height * L - T.zmin_layer[L]) / I.deltax);
+            else if (pos == 4) {
+                if (T.raw[i] > TL.at(Z).at(X - lx).at(Y - ly)) {
+                    TL[Z][X - lx][Y - ly] = T.raw[i];
+                    if (T.raw[i] < small)
+                        small = T.raw[i];
+                }
+                else
+                    i = i + 1;
+            }
+            else if (pos == 5) {
+                CR.at(Z).at(X - lx).at(Y - ly) = T.raw[i];
+                float sol = TL[Z][X - lx][Y - ly] + I.freezing / CR[Z][X - lx][Y - ly];
+                if (sol > large)
+                    large = sol;
+            }
+        }
+        T.finish[L] = round((large - small) / I.deltat);
+        if (ratio != 1) {
+            for (int k = 0; k < nzt; k++) {
+                int LowZ = k - (k % ratio), HighZ = LowZ + ratio;
+                double FHighZ = (double)(k - LowZ) / (double)(ratio), FLowZ = 1.0 - FHighZ;
+                if (HighZ > nzt - 1)
+                    HighZ = LowZ;
+                for (int i = 0; i <= ux - lx; i++) {
+                    int LowX = i - (i % ratio), HighX = LowX + ratio;
+                    double FHighX = (double)(i - LowX) / (double)(ratio), FLowX = 1.0 - FHighX;
+                    if (HighX >= ux - lx)
+                        HighX = ux - lx;
+                    for (int j = 0; j <= uy - ly; j++) {
+                        int LowY = j - (j % ratio), HighY = LowY + ratio;
+                        double FHighY = (float)(j - LowY) / (float)(ratio), FLowY = 1.0 - FHighY;
+                        if (HighY >= uy - ly)
+                            HighY = uy - ly;
+                        for (auto *A : {&TL, &CR}) {
+                            auto &V = *A;
+                            double Pt1 = V[LowZ][LowX][LowY], Pt2 = V[LowZ][HighX][LowY];
+                            double Pt12 = FLowX * Pt1 + FHighX * Pt2;
+                            double Pt3 = V[LowZ][LowX][HighY], Pt4 = V[LowZ][HighX][HighY];
+                            double Pt34 = FLowX * Pt3 + FHighX * Pt4;
+                            double Pt1234 = Pt12 * FLowY + Pt34 * FHighY;
+                            double Pt5 = V[HighZ][LowX][LowY], Pt6 = V[HighZ][HighX][LowY];
+                            double Pt56 = FLowX * Pt5 + FHighX * Pt6;
+                            double Pt7 = V[HighZ][LowX][HighY], Pt8 = V[HighZ][HighX][HighY];
+                            double Pt78 = FLowX * Pt7 + FHighX * Pt8;
+                            double Pt5678 = Pt56 * FLowY + Pt78 * FHighY;
+                            if ((Pt1 > 0) && (Pt2 > 0) && (Pt3 > 0) && (Pt4 > 0) && (Pt5 > 0) && (Pt6 > 0) && (Pt7 > 0) &&
+                                (Pt8 > 0))
+                                V[k][i][j] = Pt1234 * FLowZ + Pt5678 * FHighZ;
+                        }
+                    }
+                }
+            }
+        }
+        if (L == 0) {
+            ZBound_High = round((T.zmin_layer[0] - T.ZMin) / I.deltax) + 2 + nzt - 1;
+            nzActive = ZBound_High + 1;
+        }
+        for (int k = 0; k < nzt; k++)
+            for (int ii = lx; ii <= ux; ii++)
+                for (int jj = ly; jj <= uy; jj++) {
+                    double CTLiq = TL[k][ii - lx][jj - ly] - small;
+                    if (CTLiq > 0) {
+                        int ZOffset = round((T.zmin_layer[L] - T.ZMin) / I.deltax) + k + 2;
+                        long p = (long)ZOffset * MX * MY + (long)(ii + 1) * MY + (jj + 1);
+                        CTS.at(p) = round(CTLiq / I.deltat);
+                        Layer[p] = L;
+                        DU[p] = std::abs(CR[k][ii - lx][jj - ly]) * I.deltat;
+                    }
+                }
+    }
 }
 
 // ---- state ---------------------------------------------------------------------------------------
@@ -156,6 +384,7 @@ struct Oracle {
     std::vector<int> NucleiLocation, NucleationTimes;
     double A, B, C, D;
     int cycle = 0, nn = 0, layer = 0;
+    std::vector<int> finish; // type R: per layer, FinishTimeStep
     std::vector<int> SteeringVector;
 
     long idx(int k, int i, int j) const { return (long)k * MX * MY + (long)i * MY + j; }
@@ -266,8 +495,11 @@ void fresh_octahedron(Oracle &o, long D3D1, int GlobalX, int GlobalY, int Global
 }
 
 void initialise(Oracle &o) {
-    const Input &I = o.in;
+    Input &I = o.in;
     neighbour_tables(o);
+    TemperatureGrid T;
+    if (I.type == "R")
+        mesh_reduced(I, T);
     o.MX = I.nx + 2;
     o.MY = I.ny + 2;
     o.nz = I.nz;
@@ -292,6 +524,10 @@ void initialise(Oracle &o) {
                     o.UndercoolingChange[p] = I.R * I.deltat;
                     o.CritTimeStep[p] = (int)(((k - 1) * I.G * I.deltax) / (I.R * I.deltat));
                 }
+    }
+    else if (I.type == "R") {
+        temp_reduced(I, T, MX, MY, nz, o.CritTimeStep, o.UndercoolingChange, o.LayerID, o.ZBound_High, o.nzActive);
+        o.finish = T.finish;
     }
     else {
         // src/CAinitialize.cpp:1058-1124
@@ -406,14 +642,18 @@ void initialise(Oracle &o) {
         for (long p = (long)MX * MY * o.nzActive; p < o.N; p++)
             if (o.CritTimeStep[p] == 0)
                 o.GrainID[p] = id++;
-        // src/CAinitialize.cpp:1736-1830
+        // src/CAinitialize.cpp:1736-1830 (with the extra wall ring of type R inputs that ask for it)
         for (int k = 0; k < nz; k++)
             for (int i = 0; i < MX; i++)
-                for (int j = 0; j < MY; j++)
-                    if (is_wall(i, j, k)) {
+                for (int j = 0; j < MY; j++) {
+                    const int gx = i + o.XOff, gy = j + o.YOff;
+                    const bool extra = I.extra_walls && (gx == 0 || gx == nxg - 1 || gy == 0 || gy == nyg - 1 ||
+                                                         gx == 1 || gx == nxg - 2 || gy == 1 || gy == nyg - 2);
+                    if (is_wall(i, j, k) || extra) {
                         o.CellType[o.idx(k, i, j)] = Wall;
                         o.GrainID[o.idx(k, i, j)] = 0;
                     }
+                }
         for (int k = 1; k < nz - 1; k++)
             for (int j = 0; j < MY; j++)
                 for (int i = 0; i < MX; i++)
@@ -658,7 +898,7 @@ int check(Oracle &o) {
         }
     if (sh + uc == 0)
         return 1;
-    if (o.in.type == "S" && uc == 0) {
+    if ((o.in.type == "S" || o.in.type == "R") && uc == 0) {
         unsigned long next = (unsigned long)-1;
         for (long D3D1 = 0; D3D1 < o.NA; D3D1++) {
             long g = D3D1 + (long)o.ZBound_Low * o.MX * o.MY;
@@ -668,6 +908,9 @@ int check(Oracle &o) {
         }
         if ((next - o.cycle) > 5000)
             o.cycle = next - 1;
+        // src/CAupdate.cpp:818-819
+        if (o.in.type == "R" && o.cycle >= o.finish[o.layer])
+            return 1;
     }
     return 0;
 }

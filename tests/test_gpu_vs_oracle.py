@@ -1,11 +1,12 @@
 """GPU solver vs the CPU restatement oracle on seeded random problems of both kinds: identical
 CellType, GrainID and DiagonalLength after the same raw cycle counts, and identical final state and
 cycle at termination (bit-exact; the arithmetic is integer and reference-order floating point),
-single-layer and multilayer (the active window moved between layers)."""
+single-layer and multilayer (the active window moved between layers), and with temperatures read
+from seeded random temperature files (type R: interpolation, file series, several cooling rates)."""
 import numpy as np
 import pytest
 
-from gen_inputs import random_c, random_s
+from gen_inputs import random_c, random_r, random_s
 from oracle_port import Oracle
 
 import exaca_b200 as ex
@@ -77,6 +78,20 @@ def test_spot_melt_multilayer_random_to_termination(lib, tmp_path, seed):
     assert st.layer == int(open(inp).read().split("Number of layers:")[1].split()[0]) - 1
     o.fields()  # refreshes the oracle's window geometry
     assert (st.window_nz, st.window_nz * p.geometry.mx * p.geometry.my) == (o.nz_active, o.na)
+    compare(pool, slot, o, "final")
+    pool.close()
+
+
+@pytest.mark.parametrize("seed", range(10))
+def test_temperature_files_random_to_termination(lib, tmp_path, seed):
+    inp = random_r(5000 + seed, str(tmp_path))
+    p = ex.Problem.from_file(inp)
+    o = Oracle(inp)
+    pool = ex.Pool(0, list_capacity=p.geometry.domain_size)
+    slot = pool.admit(p, device_check=False)
+    compare(pool, slot, o, "after init")
+    assert pool.run_plain(slot) == o.run()
+    o.fields()
     compare(pool, slot, o, "final")
     pool.close()
 

@@ -14,13 +14,7 @@ def sha(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
 
-def restated(case):
-    """The restatement covers problem types C and S; type-R cases are pinned by the golden fixtures
-    of the reference's own runs alone."""
-    return "Problem type: R" not in open(input_path(case)).read()
-
-
-@pytest.mark.parametrize("case", [c for c in golden_cases() if restated(c)])
+@pytest.mark.parametrize("case", golden_cases())
 def test_oracle_matches_reference(case):
     g = load_golden(case)
     o = Oracle(input_path(case))
