@@ -401,6 +401,8 @@ __device__ __noinline__ void begin_lists(PoolState *P) {
         P->tomb_s[lane].v = 0;
         P->qcnt_s[lane].v = 0;
         P->tcnt_s[lane].v = 0;
+        if (lane == 0)
+            P->claim_overflow = 0;
 #pragma unroll
         for (int o = 16; o; o >>= 1)
             added += __shfl_down_sync(0xffffffffu, added, o);
@@ -652,11 +654,18 @@ __device__ __forceinline__ unsigned long long warp_reserve_n(unsigned long long 
 
 // Claim work of queue entry k. Returns the directions of the cells it claimed. All loads of the entry
 // (critical-length row, neighbour types) go out in one round.
-__device__ __forceinline__ unsigned int claim_entry(PoolState *P, ActiveRec *recs, unsigned long long k,
-                                                    CycleStats &st, unsigned long long &tombs) {
-    const unsigned int i = __ldcg(P->qpos + k), c = __ldcg(P->qcell + k), dom = __ldcg(P->qdom + k);
-    unsigned int m = __ldcg(P->qmask + k);
-    const float dl = __ldcg(P->qdl + k);
+// A record the growth pass flagged for a claim step: its list position, cell, domain, liquid mask
+// and grown DiagonalLength.
+struct ClaimItem {
+    unsigned int pos, cell, dom, mask;
+    float dl;
+};
+
+__device__ __forceinline__ unsigned int claim_record(PoolState *P, ActiveRec *recs, const ClaimItem &it,
+                                                     CycleStats &st, unsigned long long &tombs) {
+    const unsigned int i = it.pos, c = it.cell, dom = it.dom;
+    unsigned int m = it.mask;
+    const float dl = it.dl;
     DomainDesc &D = P->desc[dom];
     const int plane = D.mx * D.my, my = D.my;
     // the 26 critical lengths as 13 aligned 8-byte loads (26 * 4 * c is 8-byte aligned)
@@ -732,6 +741,43 @@ __device__ __forceinline__ unsigned int claim_entry(PoolState *P, ActiveRec *rec
     return reach;
 }
 
+// The claim step of global claim-queue entry k.
+__device__ __forceinline__ unsigned int claim_entry(PoolState *P, ActiveRec *recs, unsigned long long k,
+                                                    CycleStats &st, unsigned long long &tombs) {
+    const ClaimItem it{__ldcg(P->qpos + k), __ldcg(P->qcell + k), __ldcg(P->qdom + k), __ldcg(P->qmask + k),
+                       __ldcg(P->qdl + k)};
+    return claim_record(P, recs, it, st, tombs);
+}
+
+// Lists the claims of one record per lane (all lanes of the warp call; reach 0: none) for the
+// capture pass, as (domain << 37) | (direction << 32) | claimed cell, in shard `shard`.
+__device__ __forceinline__ void list_claims(PoolState *P, unsigned int shard, unsigned int reach, unsigned int dom,
+                                            unsigned int cell) {
+    const unsigned long long cap = P->shard_cap;
+    unsigned long long pos = warp_reserve_n(&P->tcnt_s[shard].v, cap, &P->error, __popc(reach));
+    if (reach && pos != ULLONG_MAX) {
+        pos += (unsigned long long)shard * cap;
+        const DomainDesc &D = P->desc[dom];
+        const int plane = D.mx * D.my, my = D.my;
+        unsigned long long t = pos;
+        for (unsigned int bits = reach; bits; bits &= bits - 1) {
+            const int l = __ffs(bits) - 1;
+            P->tgt[t++] = ((unsigned long long)dom << 37) | ((unsigned long long)l << 32) |
+                          (unsigned int)((long long)cell + nb_offset(l, plane, my));
+        }
+    }
+}
+
+// The flagged records of a block wait in shared memory for the block's own claim step, which starts
+// as soon as the block has grown its records (no grid-wide wait between growth and claims). A
+// block that flags more than kBlockQueue records in a cycle sends the rest to the global queue,
+// whose claim pass then runs after a grid-wide barrier (a flag tells every block).
+constexpr int kBlockQueue = 640;
+struct BlockQueue {
+    ClaimItem *items;    // kBlockQueue entries in shared memory
+    unsigned int *count; // in shared memory; may exceed kBlockQueue (the excess went global)
+};
+
 // Puts the flagged records of one growth step into the claim queue (all lanes of the warp call).
 template <int kBatch>
 __device__ __forceinline__ void queue_flagged(PoolState *P, unsigned int shard, unsigned int nf, unsigned int flagged,
@@ -754,10 +800,85 @@ __device__ __forceinline__ void queue_flagged(PoolState *P, unsigned int shard, 
     }
 }
 
+// Puts the flagged records of one growth step into the block's queue; those that do not fit go to
+// the global queue (all lanes of the warp call). Every slot below kBlockQueue that a warp reserves
+// is written in the same step, so the block's claim step reads only this cycle's records.
+template <int kBatch>
+__device__ __forceinline__ void block_queue_flagged(PoolState *P, BlockQueue bq, unsigned int shard, unsigned int nf,
+                                                    unsigned int flagged, const unsigned long long *idx,
+                                                    const ActiveRec *r, const unsigned int *dom, const unsigned int *m) {
+    const unsigned int lane = threadIdx.x & 31;
+    unsigned int incl = nf;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const unsigned int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= (unsigned)o)
+            incl += v;
+    }
+    const unsigned int total = __shfl_sync(0xffffffffu, incl, 31);
+    unsigned int base = 0;
+    if (lane == 31 && total)
+        base = atomicAdd(bq.count, total);
+    base = __shfl_sync(0xffffffffu, base, 31);
+    const unsigned int first = base + incl - nf; // this lane's first slot
+    unsigned int e = first, n_global = 0;
+#pragma unroll
+    for (int q = 0; q < kBatch; q++)
+        if (flagged & (1u << q)) {
+            if (e < (unsigned int)kBlockQueue)
+                bq.items[e] = ClaimItem{(unsigned int)idx[q], r[q].cell, dom[q], m[q], r[q].dl};
+            else
+                n_global++;
+            e++;
+        }
+    if (__any_sync(0xffffffffu, n_global != 0)) {
+        if (lane == 0)
+            P->claim_overflow = 1;
+        unsigned long long k = warp_reserve_n(&P->qcnt_s[shard].v, P->shard_cap, &P->error, n_global);
+        if (n_global && k != ULLONG_MAX) {
+            k += (unsigned long long)shard * P->shard_cap;
+            e = first;
+#pragma unroll
+            for (int q = 0; q < kBatch; q++)
+                if (flagged & (1u << q)) {
+                    if (e >= (unsigned int)kBlockQueue) {
+                        P->qpos[k] = (unsigned int)idx[q];
+                        P->qcell[k] = r[q].cell;
+                        P->qdom[k] = dom[q];
+                        P->qmask[k] = m[q];
+                        P->qdl[k] = r[q].dl;
+                        k++;
+                    }
+                    e++;
+                }
+        }
+    }
+}
+
+// The block's claim step over its queue (all threads of the block call, after the block's growth).
+__device__ __forceinline__ void block_claims(PoolState *P, BlockQueue bq, unsigned int shard, CycleStats &st,
+                                             unsigned long long &tombs) {
+    __syncthreads();
+    const unsigned int n = min(*bq.count, (unsigned int)kBlockQueue);
+    ActiveRec *recs = P->rec[P->pending];
+    const unsigned int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (unsigned int k0 = warp * 32; k0 < n; k0 += kBlock) {
+        const unsigned int k = k0 + lane;
+        unsigned int reach = 0, dom = 0, cell = 0;
+        if (k < n) {
+            const ClaimItem it = bq.items[k];
+            reach = claim_record(P, recs, it, st, tombs);
+            dom = it.dom;
+            cell = it.cell;
+        }
+        list_claims(P, shard, reach, dom, cell);
+    }
+}
+
 // Growth step of a compaction cycle: the survivors are written to the other list (rare; kept out of
 // line).
 __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long long gw, unsigned long long nw,
-                                         unsigned long long n, CycleStats &st) {
+                                         unsigned long long n, CycleStats &st, const BlockQueue *bq) {
     const unsigned int lane = threadIdx.x & 31;
     DomainDesc *desc = P->desc;
     const bool extras = P->extras;
@@ -804,7 +925,11 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
         }
         const bool flag = placed && __float_as_uint(r.cdl_min) == kNeedsClaim;
         unsigned long long idx = pos;
-        queue_flagged<1>(P, (unsigned int)(gw % kShards), flag ? 1u : 0u, flag ? 1u : 0u, &idx, &r, &dom, &m);
+        if (bq)
+            block_queue_flagged<1>(P, *bq, (unsigned int)(gw % kShards), flag ? 1u : 0u, flag ? 1u : 0u, &idx, &r,
+                                   &dom, &m);
+        else
+            queue_flagged<1>(P, (unsigned int)(gw % kShards), flag ? 1u : 0u, flag ? 1u : 0u, &idx, &r, &dom, &m);
     }
 }
 
@@ -812,14 +937,27 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
 // group g to warp g % (number of warps of the grid), consecutive warps on different blocks: the
 // records appended by the last capture pass, which all need a fresh mask and claims, spread over
 // every SM. No block-wide synchronisation.
-template <int kBatch> __device__ void grow_pass(PoolState *P, CycleStats &st) {
+template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P, CycleStats &st) {
     const int cur = P->cur;
     const unsigned long long n = P->cnt[cur];
     const unsigned int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const unsigned long long nw = (unsigned long long)gridDim.x * (kBlock / 32);
     const unsigned long long gw = (unsigned long long)warp * gridDim.x + blockIdx.x;
+    const unsigned int shard = (unsigned int)(gw % kShards);
+    __shared__ ClaimItem s_items[kBlockClaims ? kBlockQueue : 1];
+    __shared__ unsigned int s_count;
+    const BlockQueue bq{s_items, &s_count};
+    if (kBlockClaims) {
+        if (threadIdx.x == 0)
+            s_count = 0;
+        __syncthreads();
+    }
     if (P->compact) {
-        compact_pass(P, cur, gw, nw, n, st);
+        compact_pass(P, cur, gw, nw, n, st, kBlockClaims ? &bq : nullptr);
+        if (kBlockClaims) {
+            unsigned long long claim_tombs = 0; // a compacted list starts without dropped records
+            block_claims(P, bq, shard, st, claim_tombs);
+        }
         return;
     }
     ActiveRec *in = P->rec[cur];
@@ -884,8 +1022,13 @@ template <int kBatch> __device__ void grow_pass(PoolState *P, CycleStats &st) {
                     flagged |= 1u << q;
             }
         }
-        queue_flagged<kBatch>(P, (unsigned int)(gw % kShards), __popc(flagged), flagged, idx, r, dom, m);
+        if (kBlockClaims)
+            block_queue_flagged<kBatch>(P, bq, shard, __popc(flagged), flagged, idx, r, dom, m);
+        else
+            queue_flagged<kBatch>(P, shard, __popc(flagged), flagged, idx, r, dom, m);
     }
+    if (kBlockClaims)
+        block_claims(P, bq, shard, st, tombs);
     // dropped records stay as tombstones of the in-place list until the next compaction
 #pragma unroll
     for (int o = 16; o; o >>= 1)
@@ -944,19 +1087,7 @@ __device__ void claim_pass(PoolState *P, CycleStats &st) {
             dom = __ldcg(P->qdom + e);
             cell = __ldcg(P->qcell + e);
         }
-        const unsigned int ts = (unsigned int)(gw % kShards);
-        unsigned long long pos = warp_reserve_n(&P->tcnt_s[ts].v, cap, &P->error, __popc(reach));
-        if (reach && pos != ULLONG_MAX) {
-            pos += (unsigned long long)ts * cap;
-            const DomainDesc &D = P->desc[dom];
-            const int plane = D.mx * D.my, my = D.my;
-            unsigned long long t = pos;
-            for (unsigned int bits = reach; bits; bits &= bits - 1) {
-                const int l = __ffs(bits) - 1;
-                P->tgt[t++] = ((unsigned long long)dom << 37) | ((unsigned long long)l << 32) |
-                              (unsigned int)((long long)cell + nb_offset(l, plane, my));
-            }
-        }
+        list_claims(P, (unsigned int)(gw % kShards), reach, dom, cell);
     }
     if (!P->compact) {
 #pragma unroll
@@ -1113,7 +1244,7 @@ __device__ void finish_capture(PoolState *P) {
 
 template <int kBatch> __global__ void __launch_bounds__(kBlock) k_grow(PoolState *P) {
     CycleStats st;
-    grow_pass<kBatch>(P, st);
+    grow_pass<kBatch, false>(P, st);
     flush_stats(P, st);
 }
 
@@ -1241,14 +1372,18 @@ template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 2) k
         ok = grid_meet(P, -1, [] {});
     }
     for (int c = 0; ok && c < n_cycles; c++) {
-        grow_pass<kBatch>(P, st);
+        // growth with each block's claims right after its own growth; the global claim pass only
+        // when some block's queue overflowed this cycle (the same answer for every block)
+        grow_pass<kBatch, true>(P, st);
         ok = grid_meet(P, 3 * c + 1, [] {});
         if (!ok)
             break;
-        claim_pass(P, st);
-        ok = grid_meet(P, 3 * c + 2, [] {});
-        if (!ok)
-            break;
+        if (__ldcg(&P->claim_overflow)) {
+            claim_pass(P, st);
+            ok = grid_meet(P, 3 * c + 2, [] {});
+            if (!ok)
+                break;
+        }
         capture_pass<kLanes>(P, st);
         const bool more = c + 1 < n_cycles;
         ok = grid_meet(P, 3 * c + 3, [&] {
@@ -2245,16 +2380,21 @@ void Pool::profile_persistent(int n, double us[7]) {
     CUDA_OK(cudaMemcpyAsync(tl.data(), dtl, words * sizeof(unsigned long long), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
     CUDA_OK(cudaFree(dtl));
-    // meeting points 3c+1, 3c+2, 3c+3 close cycle c's growth, claim and capture passes
+    // meeting points 3c+1, 3c+2, 3c+3 close cycle c's growth (with the blocks' own claims), global
+    // claim and capture passes; 3c+2 is skipped (all zero) in cycles without a queue overflow
     for (int c = 0; c < n; c++) {
         const unsigned long long *prev = &tl[3 * (3 * c)], *m1 = &tl[3 * (3 * c + 1)], *m2 = &tl[3 * (3 * c + 2)],
                                  *m3 = &tl[3 * (3 * c + 3)];
         us[0] += (double)(m1[0] - prev[2]);
         us[1] += (double)(m1[1] - prev[2]);
-        us[2] += (double)(m2[0] - m1[2]);
-        us[3] += (double)(m2[1] - m1[2]);
-        us[4] += (double)(m3[0] - m2[2]);
-        us[5] += (double)(m3[1] - m2[2]);
+        const unsigned long long *before_capture = m1;
+        if (m2[2]) {
+            us[2] += (double)(m2[0] - m1[2]);
+            us[3] += (double)(m2[1] - m1[2]);
+            before_capture = m2;
+        }
+        us[4] += (double)(m3[0] - before_capture[2]);
+        us[5] += (double)(m3[1] - before_capture[2]);
         us[6] += (double)(m3[2] - m3[1]);
     }
     for (int k = 0; k < 7; k++)

@@ -139,6 +139,8 @@ struct PoolState {
     int error;
     int n_domains;
     int extras; // 1 once a domain with per-cell growth extras (several layers or undercooling values) was admitted
+    int claim_overflow; // 1: a block's claim queue overflowed this cycle, so the global claim pass runs
+    int pad;
     DomainDesc *desc;
     unsigned long long stat[kStatShards][kNumStats];
     unsigned int blocks_done;      // last-block detection of the separate capture kernel

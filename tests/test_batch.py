@@ -65,3 +65,16 @@ def test_retiring_a_running_domain(lib):
         assert same(res, plain, 0, 0) and same(res, plain, 1, 2)
     finally:
         pool.close()
+
+
+@pytest.mark.gpu
+def test_batch_with_crowded_first_cycles(lib):
+    # ~240k substrate seeds need their first claim step in the first cycle, more than the blocks'
+    # shared-memory claim queues hold, so part of the claims go through the global queue; every
+    # domain must still equal its own plain run (where that does not happen)
+    probs = [ex.Problem.directional(254, 254, 6 + q, G=5e6, R=1e5, n_ratio=25, nucleation_density=50.0,
+                                    fract_surface_active=0.9) for q in range(4)]
+    plain = batch.solve_plain(probs)
+    res = batch.solve_batch(probs, config=0)
+    for i in range(len(probs)):
+        assert same(res, plain, i), f"domain {i} differs from its plain run"
