@@ -832,8 +832,6 @@ __device__ __forceinline__ void block_queue_flagged(PoolState *P, BlockQueue bq,
             e++;
         }
     if (__any_sync(0xffffffffu, n_global != 0)) {
-        if (lane == 0)
-            P->claim_overflow = 1;
         unsigned long long k = warp_reserve_n(&P->qcnt_s[shard].v, P->shard_cap, &P->error, n_global);
         if (n_global && k != ULLONG_MAX) {
             k += (unsigned long long)shard * P->shard_cap;
@@ -859,6 +857,10 @@ __device__ __forceinline__ void block_queue_flagged(PoolState *P, BlockQueue bq,
 __device__ __forceinline__ void block_claims(PoolState *P, BlockQueue bq, unsigned int shard, CycleStats &st,
                                              unsigned long long &tombs) {
     __syncthreads();
+    // one store per block: every warp of the grid storing to this flag once its block's queue was
+    // full serialised on one L2 slice
+    if (threadIdx.x == 0 && *bq.count > (unsigned int)kBlockQueue)
+        P->claim_overflow = 1;
     const unsigned int n = min(*bq.count, (unsigned int)kBlockQueue);
     ActiveRec *recs = P->rec[P->pending];
     const unsigned int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
