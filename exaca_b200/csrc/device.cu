@@ -364,54 +364,62 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     return (float)NewODiagL;
 }
 
-// A nucleation site stopped being liquid: its active neighbours drop it from their masks. The 26
-// neighbour types are loaded first (invalid directions read the site itself), then the updates go out.
-__device__ void drop_from_neighbour_masks(const DomainDesc &D, unsigned int *rstat, unsigned long long cap,
-                                          unsigned int t) {
-    int rx, ry, rz;
-    cell_coords(D, t, rx, ry, rz);
-    const unsigned int valid = neighbour_mask(D, rx, ry, rz);
-    const int plane = D.mx * D.my, my = D.my;
-    int8_t nt[26];
-    unsigned int np[26];
-#pragma unroll
-    for (int l = 0; l < 26; l++) {
-        const long long a = (long long)t + ((valid >> l) & 1u ? nb_offset(l, plane, my) : 0);
-        nt[l] = __ldcg(D.ctype + a);
-        np[l] = __ldcg(D.pos + a);
-    }
-#pragma unroll
-    for (int l = 0; l < 26; l++)
-        if (((valid >> l) & 1u) && nt[l] == kActive && np[l] < cap)
-            atomicAnd(rstat + np[l], ~(1u << c_opp[l]));
-}
-
 // ---------------------------------------------------------------------------------------------
-// Start of a CA cycle for every domain (src/runCA.cpp:290-298, src/CAupdate.cpp:67-200), run by one
-// block: list swap, device-side termination check, cycle advance, nucleation. Reads that may see
-// data other blocks of the same kernel wrote go through L2 (__ldcg).
-// Start of a cycle, pool part (one warp): list swap, compaction decision, per-cycle counters.
-__device__ __noinline__ void begin_lists(PoolState *P) {
+// Start of a CA cycle (src/runCA.cpp:290-298, src/CAupdate.cpp:67-200): list swap, device-side
+// termination check, cycle advance, nucleation. In the persistent kernel the start of a few domains
+// runs in one block while the rest of the grid waits, so its cost is its chain of dependent round
+// trips to L2 / HBM. Every load that does not depend on an earlier one goes out in the same round:
+//   1. the pool's list counters, and each domain's descriptor fields;
+//   2. the next 32 nucleation sites by time, with the rest of the descriptor;
+//   3. per due site: its CellType, LayerID, GrainID and CritTimeStep;
+//   4. per firing site, with the whole warp: its critical-length row and its neighbours' CellTypes and
+//      list positions (the list slots of all firing sites are reserved under the first such round).
+// Reads that may see data other blocks of the same kernel wrote go through L2 (__ldcg).
+
+// Pool part (warp 0): when `close`, the records the last capture pass appended join the list the
+// next cycle reads, which ends the previous cycle; then the list swap, the compaction decision and
+// the per-cycle counters. One round of loads. The list this cycle reads goes to *cur_out if given.
+__device__ __forceinline__ void lists_start(PoolState *P, bool close, int *cur_out) {
     if (threadIdx.x < 32) {
-        // the list the previous cycle left becomes current; when it was a compacted copy, the old
-        // one is emptied and carries no dropped records any more (all loads issued together)
         static_assert(kShards == 32, "one lane per shard");
         const int lane = threadIdx.x;
-        unsigned long long added = P->tomb_s[lane].v;
+        unsigned long long added = __ldcg(&P->tomb_s[lane].v);
+        unsigned long long appended = close ? __ldcg(&P->tcnt_s[lane].v) : 0ull;
+        int prev = 0, cur = 0;
+        unsigned long long cnt0 = 0, cnt1 = 0, tombs = 0, cap = 0;
+        if (lane == 0) {
+            prev = __ldcg(&P->cur);
+            cur = __ldcg(&P->pending);
+            cnt0 = __ldcg(&P->cnt[0]);
+            cnt1 = __ldcg(&P->cnt[1]);
+            tombs = __ldcg(&P->tombs);
+            cap = P->capacity;
+        }
         P->tomb_s[lane].v = 0;
         P->qcnt_s[lane].v = 0;
         P->tcnt_s[lane].v = 0;
-        if (lane == 0)
-            P->claim_overflow = 0;
 #pragma unroll
-        for (int o = 16; o; o >>= 1)
+        for (int o = 16; o; o >>= 1) {
             added += __shfl_down_sync(0xffffffffu, added, o);
+            appended += __shfl_down_sync(0xffffffffu, appended, o);
+        }
         if (lane == 0) {
-            const int prev = P->cur;
-            const int cur = P->pending;
-            const unsigned long long cnt0 = P->cnt[0], cnt1 = P->cnt[1];
-            unsigned long long tombs = P->tombs + added;
+            P->claim_overflow = 0;
+            if (close) {
+                // the capture pass reserved its new records' slots past the count of list `cur`
+                const unsigned long long grown = (cur ? cnt1 : cnt0) + appended;
+                if (grown <= cap) {
+                    if (cur)
+                        cnt1 = grown;
+                    else
+                        cnt0 = grown;
+                    P->cnt[cur] = grown;
+                }
+            }
+            // the list the previous cycle left becomes current; when it was a compacted copy, the old
+            // one is emptied and carries no dropped records any more
             const unsigned long long cnt_cur = cur ? cnt1 : cnt0;
+            tombs += added;
             if (cur != prev) {
                 P->cnt[prev] = 0;
                 tombs = 0;
@@ -419,116 +427,211 @@ __device__ __noinline__ void begin_lists(PoolState *P) {
             P->tombs = tombs;
             P->cur = cur;
             // compact when dropped records exceed an eighth of the list
-            int compact = tombs * 8 > cnt_cur ? 1 : 0;
+            const int compact = tombs * 8 > cnt_cur ? 1 : 0;
             P->compact = compact;
             P->pending = compact ? cur ^ 1 : cur;
             if (compact)
                 P->cnt[cur ^ 1] = 0;
+            if (cur_out)
+                *cur_out = cur;
         }
     }
 }
 
-// Start of a cycle, per-domain part: warps first_warp, first_warp + warp_stride, ... take one
-// domain each (the current list must already be settled by begin_lists).
-__device__ __noinline__ void begin_domains(PoolState *P, int first_warp, int warp_stride) {
-    const int cur = P->cur;
-    const int lane = threadIdx.x & 31;
-    unsigned long long nucleated = 0;
-    const int n_domains = P->n_domains;
-    DomainDesc *const desc = P->desc;
-    for (int d = first_warp; d < n_domains; d += warp_stride) {
-        DomainDesc &D = desc[d];
-        // Every field the start reads, and the first 32 nuclei from the cursor, in one round of
-        // loads: this runs while the rest of the grid waits, so its dependent chain is the cost.
-        const int8_t *const ctype = D.ctype;
-        const int done = D.done, check_mode = D.check_mode, cycle0 = D.cycle, cursor0 = D.nuc_cursor;
-        const int n_nuclei = D.n_nuclei, layer_no = D.layer_no, nn0 = D.nn;
-        const unsigned int epoch0 = D.epoch;
-        const long long liquid0 = D.liquid, active_size = D.active_size;
-        const int32_t *const nuc_time = D.nuc_time, *const nuc_loc = D.nuc_loc;
-        if (ctype == nullptr || done)
-            continue;
-        int idx = cursor0 + lane;
-        int t = idx < n_nuclei ? __ldg(nuc_time + idx) : INT_MAX;
-        int l = idx < n_nuclei ? __ldg(nuc_loc + idx) : -1;
-        __syncwarp(); // every lane has read the cycle before lane 0 advances it
-        if (check_mode && cycle0 > 0 && cycle0 % 1000 == 0 && domain_liquid(D) == 0) {
-            // src/CAupdate.cpp:782-783: no superheated or undercooled liquid left
-            if (lane == 0)
-                D.done = 1;
-            continue;
-        }
-        const int cycle = cycle0 + 1;
-        if (lane == 0) {
-            D.cycle = cycle;
-            D.epoch = epoch0 + 1;
-        }
-        // src/CAupdate.cpp:76-198: sites with cycle >= NucleationTimes that are still liquid
-        int cursor = cursor0;
-        int fired_total = 0;
-        while (true) {
-            unsigned int due = __ballot_sync(0xffffffffu, t <= cycle);
-            // nuclei are sorted by time, so the due ones form a prefix
-            int n_due = __popc(due);
-            bool fire = false;
-            unsigned int loc = 0;
-            if (t <= cycle) {
-                if (l < 0 || l >= active_size) {
-                    atomicOr(&D.error, kErrBounds);
-                }
-                else {
-                    loc = (unsigned int)l;
-                    fire = __ldcg(ctype + loc) == kLiquid && D.layer[loc] <= layer_no;
-                }
+__device__ __noinline__ void begin_lists(PoolState *P, bool close) { lists_start(P, close, nullptr); }
+
+// Descriptor fields of the first round (the cursor into the nucleation sites and what decides
+// whether the domain runs this cycle).
+struct DomainStart {
+    const int32_t *nuc_time, *nuc_loc;
+    int8_t *ctype;
+    int done, check_mode, cycle0, cursor0, n_nuclei;
+};
+
+__device__ __forceinline__ DomainStart load_start(const DomainDesc &D) {
+    DomainStart s;
+    s.nuc_time = D.nuc_time;
+    s.nuc_loc = D.nuc_loc;
+    s.ctype = D.ctype;
+    s.n_nuclei = D.n_nuclei;
+    s.check_mode = D.check_mode;
+    s.done = __ldcg(&D.done);
+    s.cycle0 = __ldcg(&D.cycle);
+    s.cursor0 = __ldcg(&D.nuc_cursor);
+    return s;
+}
+
+// Cycle start of domain d by one warp (all lanes call with the same arguments).
+__device__ __forceinline__ void start_domain(PoolState *P, DomainDesc &D, const DomainStart &s, unsigned int d,
+                                             int cur, unsigned long long &nucleated) {
+    const unsigned int lane = threadIdx.x & 31;
+    if (s.ctype == nullptr || s.done)
+        return;
+    if (s.check_mode && s.cycle0 > 0 && s.cycle0 % 1000 == 0 && domain_liquid(D) == 0) {
+        // src/CAupdate.cpp:782-783: no superheated or undercooled liquid left
+        if (lane == 0)
+            D.done = 1;
+        return;
+    }
+    const int cycle = s.cycle0 + 1;
+    int cursor = s.cursor0, fired_total = 0;
+    // round 2: the rest of the descriptor goes out with the first batch of sites
+    const int8_t *const layer = D.layer;
+    int32_t *const gid = D.gid;
+    const int32_t *const cts_run = D.cts_run;
+    float *const dl = D.dl, *const doc = D.doc, *const cdl = D.cdl;
+    const float *const cdl_table = D.cdl_table;
+    unsigned int *const pos = D.pos;
+    const int layer_no = D.layer_no, mx = D.mx, my = D.my, z_end = D.z_end, xoff = D.xoff, yoff = D.yoff;
+    const long long active_size = D.active_size;
+    const unsigned int epoch0 = __ldcg(&D.epoch);
+    const int nn0 = __ldcg(&D.nn);
+    const long long liquid0 = __ldcg(&D.liquid);
+    const unsigned long long cap = P->capacity;
+    unsigned int *const rstat = P->rstat[cur];
+    // src/CAupdate.cpp:76-198: sites with cycle >= NucleationTimes that are still liquid
+    while (cursor < s.n_nuclei) {
+        const int idx = cursor + (int)lane;
+        const int t = idx < s.n_nuclei ? __ldg(s.nuc_time + idx) : INT_MAX;
+        const int l = idx < s.n_nuclei ? __ldg(s.nuc_loc + idx) : -1;
+        const bool due = t <= cycle;
+        // sites are sorted by time, so the due ones form a prefix
+        const int n_due = __popc(__ballot_sync(0xffffffffu, due));
+        if (n_due == 0)
+            break;
+        // round 3
+        bool fire = false;
+        unsigned int loc = 0;
+        int h = 0, cts = 0;
+        if (due) {
+            if (l < 0 || l >= active_size) {
+                atomicOr(&D.error, kErrBounds);
             }
-            if (fire) {
-                make_fresh_octahedron(D, loc);
-                unsigned long long pos = warp_reserve(&P->cnt[cur], P->capacity, &P->error);
-                if (pos != ULLONG_MAX) {
+            else {
+                loc = (unsigned int)l;
+                const int8_t site_type = __ldcg(s.ctype + loc);
+                const int site_layer = layer[loc];
+                h = __ldcg(gid + loc);
+                cts = cts_run[loc];
+                fire = site_type == kLiquid && site_layer <= layer_no;
+            }
+        }
+        // list slots of the firing sites (one atomic; it completes under round 4)
+        const unsigned long long my_slot = fire ? warp_reserve(&P->cnt[cur], cap, &P->error) : ULLONG_MAX;
+        // round 4, one firing site at a time with the whole warp: lanes 0-12 copy the fresh
+        // octahedron's critical lengths (src/CAupdate.cpp:100-194), lane n < 26 reads neighbour n's
+        // type and list position (an active neighbour drops the site from its liquid mask)
+        const int plane = mx * my;
+        for (unsigned int todo = __ballot_sync(0xffffffffu, fire); todo; todo &= todo - 1) {
+            const int src = __ffs(todo) - 1;
+            const unsigned int site = __shfl_sync(0xffffffffu, loc, src);
+            const int site_gid = __shfl_sync(0xffffffffu, h, src);
+            const unsigned int z = site / (unsigned int)plane;
+            const unsigned int rem = site - z * (unsigned int)plane;
+            const int rx = (int)(rem / (unsigned int)my), ry = (int)(rem - (unsigned int)rx * (unsigned int)my),
+                      rz = (int)z;
+            const int b = (ry == 0) ? (rx == 0 ? 5 : (rx == mx - 1 ? 6 : 1))
+                                    : (ry == my - 1 ? (rx == 0 ? 7 : (rx == mx - 1 ? 8 : 2))
+                                                    : (rx == 0 ? 3 : (rx == mx - 1 ? 4 : 0)));
+            unsigned int valid = c_itmask[b];
+            if (rz + 1 >= z_end)
+                valid &= ~c_zplus;
+            if (rz - 1 < 0)
+                valid &= ~c_zminus;
+            int ori = (abs(site_gid) - 1) % 10000;
+            if (ori < 0)
+                ori += 10000;
+            float2 row = make_float2(0.0f, 0.0f);
+            if (lane < 13)
+                row = reinterpret_cast<const float2 *>(cdl_table + 26 * ori)[lane];
+            const bool nb = lane < 26 && ((valid >> lane) & 1u);
+            int8_t nb_type = kLiquid;
+            unsigned int nb_pos = 0;
+            if (nb) {
+                const long long a = (long long)site + nb_offset((int)lane, plane, my);
+                nb_type = __ldcg(s.ctype + a);
+                nb_pos = __ldcg(pos + a);
+            }
+            const unsigned long long slot = __shfl_sync(0xffffffffu, my_slot, src);
+            if (lane < 13)
+                reinterpret_cast<float2 *>(cdl + 26ull * site)[lane] = row;
+            if (lane == 0) {
+                dl[site] = 0.01f;
+                doc[3ull * site + 0] = (float)((double)(rx + xoff) + 0.5);
+                doc[3ull * site + 1] = (float)((double)(ry + yoff) + 0.5);
+                doc[3ull * site + 2] = (float)((double)rz + 0.5);
+            }
+            if (lane == (unsigned int)src) {
+                if (slot != ULLONG_MAX) {
                     ActiveRec r;
-                    r.cell = loc;
+                    r.cell = site;
                     r.dl = 0.01f;
                     r.cdl_min = 0.0f;
-                    r.cts = D.cts_run[loc];
-                    P->rec[cur][pos] = r;
-                    P->rdom[cur][pos] = (unsigned int)d;
-                    P->rstat[cur][pos] = kMaskFresh;
-                    P->rmin2[cur][pos] = kNoMin2;
-                    D.pos[loc] = (unsigned int)pos;
+                    r.cts = cts;
+                    P->rec[cur][slot] = r;
+                    P->rdom[cur][slot] = d;
+                    rstat[slot] = kMaskFresh;
+                    P->rmin2[cur][slot] = kNoMin2;
+                    pos[site] = (unsigned int)slot;
                 }
-                D.ctype[loc] = kActive;
+                s.ctype[site] = kActive;
             }
+            if (nb && nb_type == kActive && nb_pos < cap)
+                atomicAnd(rstat + nb_pos, ~(1u << c_opp[lane]));
             __syncwarp();
-            if (fire)
-                drop_from_neighbour_masks(D, P->rstat[cur], P->capacity, loc);
-            unsigned int fired = __ballot_sync(0xffffffffu, fire);
-            fired_total += __popc(fired);
-            cursor += n_due;
-            if (n_due < 32 || cursor >= n_nuclei)
-                break;
-            idx = cursor + lane;
-            t = idx < n_nuclei ? __ldg(nuc_time + idx) : INT_MAX;
-            l = idx < n_nuclei ? __ldg(nuc_loc + idx) : -1;
         }
-        if (lane == 0) {
-            D.nuc_cursor = cursor;
-            D.nn = nn0 + fired_total;
-            D.liquid = liquid0 - fired_total;
-            nucleated += fired_total;
-        }
+        fired_total += __popc(__ballot_sync(0xffffffffu, fire));
+        cursor += n_due;
+        if (n_due < 32)
+            break;
     }
-    if (lane == 0 && nucleated)
+    if (lane == 0) {
+        D.cycle = cycle;
+        D.epoch = epoch0 + 1;
+        D.nuc_cursor = cursor;
+        D.nn = nn0 + fired_total;
+        D.liquid = liquid0 - fired_total;
+        nucleated += fired_total;
+    }
+}
+
+// Cycle start, per-domain part, across the grid: warps first_warp, first_warp + warp_stride, ...
+// take one domain each (the current list was settled by begin_lists before a grid-wide meeting).
+__device__ __noinline__ void begin_domains(PoolState *P, DomainDesc *desc, int n_domains, int first_warp,
+                                           int warp_stride) {
+    const int cur = __ldcg(&P->cur);
+    unsigned long long nucleated = 0;
+    for (int d = first_warp; d < n_domains; d += warp_stride) {
+        const DomainStart s = load_start(desc[d]);
+        start_domain(P, desc[d], s, (unsigned int)d, cur, nucleated);
+    }
+    if ((threadIdx.x & 31) == 0 && nucleated)
         atomicAdd(&P->stat[0][kStatNucleated], nucleated);
 }
 
-// Start of a cycle by one block (the pool part, then every domain with the block's warps).
-__device__ __noinline__ void begin_cycle(PoolState *P) {
-    begin_lists(P);
+// Cycle start by one block: the pool part in warp 0 while every warp loads its first domain's
+// descriptor, then the domains with the block's warps. With `close` it first ends the previous
+// cycle (finish_capture).
+__device__ __noinline__ void begin_cycle(PoolState *P, bool close, DomainDesc *desc, int n_domains) {
+    __shared__ int s_cur;
+    const int w = (int)(threadIdx.x >> 5), nw = (int)(blockDim.x >> 5);
+    DomainStart s{};
+    if (w < n_domains)
+        s = load_start(desc[w]);
+    lists_start(P, close, &s_cur);
     __syncthreads();
-    begin_domains(P, threadIdx.x >> 5, blockDim.x >> 5);
+    const int cur = s_cur;
+    unsigned long long nucleated = 0;
+    for (int d = w; d < n_domains; d += nw) {
+        if (d != w)
+            s = load_start(desc[d]);
+        start_domain(P, desc[d], s, (unsigned int)d, cur, nucleated);
+    }
+    if ((threadIdx.x & 31) == 0 && nucleated)
+        atomicAdd(&P->stat[0][kStatNucleated], nucleated);
 }
 
-__global__ void k_step_begin(PoolState *P) { begin_cycle(P); }
+__global__ void k_step_begin(PoolState *P) { begin_cycle(P, false, P->desc, P->n_domains); }
 
 // ---------------------------------------------------------------------------------------------
 // One CA cycle after its start (begin_cycle) is three passes over the pool:
@@ -1274,9 +1377,10 @@ template <bool kBegin, int kLanes> __global__ void __launch_bounds__(kBlock) k_c
         __threadfence();
         if (threadIdx.x == 0)
             P->blocks_done = 0;
-        finish_capture(P);
         if (kBegin)
-            begin_cycle(P);
+            begin_cycle(P, true, P->desc, P->n_domains);
+        else
+            finish_capture(P);
     }
 }
 
@@ -1361,16 +1465,19 @@ template <class F> __device__ bool grid_meet(PoolState *P, int tag, F &&serial) 
 template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 2) k_cycles(PoolState *P, int n_cycles) {
     CycleStats st;
     // with many domains, their per-cycle start (termination, nucleation) runs across the grid
-    const bool spread = P->n_domains > kSerialDomains;
+    // (the descriptors and their number change only between launches)
+    DomainDesc *const desc = P->desc;
+    const int n_domains = P->n_domains;
+    const bool spread = n_domains > kSerialDomains;
     const int gwarp = (threadIdx.x >> 5) * gridDim.x + blockIdx.x, nwarp = gridDim.x * (kBlock / 32);
     bool ok = grid_meet(P, 0, [&] {
         if (spread)
-            begin_lists(P);
+            begin_lists(P, false);
         else
-            begin_cycle(P);
+            begin_cycle(P, false, desc, n_domains);
     });
     if (ok && spread) {
-        begin_domains(P, gwarp, nwarp);
+        begin_domains(P, desc, n_domains, gwarp, nwarp);
         ok = grid_meet(P, -1, [] {});
     }
     for (int c = 0; ok && c < n_cycles; c++) {
@@ -1389,16 +1496,15 @@ template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 2) k
         capture_pass<kLanes>(P, st);
         const bool more = c + 1 < n_cycles;
         ok = grid_meet(P, 3 * c + 3, [&] {
-            finish_capture(P);
-            if (more) {
-                if (spread)
-                    begin_lists(P);
-                else
-                    begin_cycle(P);
-            }
+            if (!more)
+                finish_capture(P);
+            else if (spread)
+                begin_lists(P, true);
+            else
+                begin_cycle(P, true, desc, n_domains);
         });
         if (ok && more && spread) {
-            begin_domains(P, gwarp, nwarp);
+            begin_domains(P, desc, n_domains, gwarp, nwarp);
             ok = grid_meet(P, -1, [] {});
         }
     }
