@@ -300,12 +300,14 @@ def b200_arm(args, rank, world, local):
     launch_bytes = sum(pass_bytes.values())
     peak, peak_kind = peaks()
     achieved = launch_bytes / (launch_ms / 1e3) / 1e9
+    # ncu DRAM bytes per cycle of k_cycles, per cube side it was captured at ("k_cycles <side> <bytes>")
     traffic = None
     traffic_file = os.path.join(ROOT, "profiles", "traffic_per_launch.txt")
     if os.path.exists(traffic_file):
         for ln in open(traffic_file):
-            if ln.startswith("k_cycles "):
-                traffic = float(ln.split()[1]) * args.profile_cycles  # the file holds DRAM bytes per cycle
+            f = ln.split()
+            if len(f) == 3 and f[0] == "k_cycles" and int(f[1]) == n:
+                traffic = float(f[2]) * args.profile_cycles
 
     # dense-equivalent effective roofline (the reference formulation's compulsory bytes per cycle)
     eff_bytes_per_update = 14.5
