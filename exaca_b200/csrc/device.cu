@@ -15,7 +15,9 @@
 //          solidification re-check.
 // Stretches of cycles run in one persistent cooperative kernel (k_cycles) whose blocks meet at
 // bounded grid-wide barriers between the passes; the last block to reach the end of a cycle
-// starts the next one. The same passes also run as separate kernels (per-pass timing).
+// starts the next one. In k_cycles each block runs the claim steps of the records it flagged right
+// after its own growth (a shared-memory queue); a grid-wide claim pass runs only in a cycle where
+// some block's queue overflowed. The same passes also run as separate kernels (per-pass timing).
 // The claim rule reproduces the Kokkos-Serial loop order exactly: serial visits active cells in
 // ascending index and captures flip Liquid to Active in place, so the capturer of a cell is the
 // lowest-index claimant, and an active cell sees a neighbour as liquid iff it was liquid at the
