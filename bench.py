@@ -16,6 +16,12 @@ construction), the solve and the GrainID/CellType download into pinned host buff
 than L2 and is rebuilt between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size S]
+                    [--cpu-ref auto|reference|port]
+
+`--impl reference` and the `cpu_baseline` time the reference's own OpenMP CPU path (built from its
+sources against single-rank shims into oracle/_ref) on bounded samples of the same workload; when
+that build is absent they time the oracle's serial restatement (oracle/_port) instead and say so
+(`cpu_baseline.kind` "port").
 
 For N > 1 (torchrun) every rank solves its own replica (the plain path has no exchange step) and
 rank 0 prints the aggregate over ranks with the max-over-ranks time.
@@ -37,6 +43,7 @@ METRIC = "cell-updates/s"
 UNIT = "cell-updates/s"
 WORKLOAD = dict(G=1e6, R=1e6, n_ratio=25, nucleation_density=100.0, dTN=3.0, dTsigma=0.5, fract_surface_active=0.02)
 REF_BENCH = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+PORT_LIB = os.path.join(ROOT, "oracle", "_port", "liboracle.so")
 
 # Algorithmic bytes of each pass per unit of work (the bytes the pass must read or write, each
 # counted once per use, no cache reuse credited):
@@ -168,26 +175,75 @@ def run_reference_sample(n, samples, cycles_per_sample, threads):
         return json.loads(line[line.index("{"):])
 
 
+def run_port_sample(n, samples, cycles_per_sample):
+    """The oracle's serial restatement of the reference (one core) on bounded samples of the
+    workload: the CPU baseline when the reference's own timing driver was not built."""
+    import ctypes
+
+    if not os.path.exists(PORT_LIB):
+        raise FileNotFoundError(PORT_LIB)
+    lib = ctypes.CDLL(PORT_LIB)
+    lib.oracle_create.restype = ctypes.c_void_p
+    lib.oracle_create.argtypes = [ctypes.c_char_p, ctypes.c_char_p]
+    lib.oracle_error.restype = ctypes.c_char_p
+    lib.oracle_geometry.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]
+    lib.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    lib.oracle_free.argtypes = [ctypes.c_void_p]
+    with tempfile.TemporaryDirectory() as d:
+        inp = os.path.join(d, "bench.txt")
+        with open(inp, "w") as f:
+            f.write(input_file_text(n))
+        t0 = time.perf_counter()
+        o = lib.oracle_create(inp.encode(), os.path.join(ROOT, "exaca_b200", "data").encode())
+        init_s = time.perf_counter() - t0
+        if not o:
+            raise RuntimeError(lib.oracle_error().decode())
+        try:
+            geo = (ctypes.c_longlong * 6)()
+            lib.oracle_geometry(o, geo)
+            times = []
+            for _ in range(samples):
+                t = time.perf_counter()
+                lib.oracle_step(o, cycles_per_sample)
+                times.append(time.perf_counter() - t)
+        finally:
+            lib.oracle_free(o)
+    return {"sample_s": times, "active_domain_cells": int(geo[5]), "cycles_per_sample": cycles_per_sample,
+            "cycles": samples * cycles_per_sample, "threads": 1, "init_s": init_s, "kind": "port"}
+
+
+def cpu_sample(kind, n, samples, cycles_per_sample, threads):
+    """Bounded samples of the reference's CPU path: its own OpenMP build when present ("reference"),
+    else the oracle's serial restatement ("port")."""
+    if kind == "reference" or (kind == "auto" and os.path.exists(REF_BENCH)):
+        res = run_reference_sample(n, samples, cycles_per_sample, threads)
+        res["kind"] = "reference"
+        return res
+    return run_port_sample(n, samples, cycles_per_sample)
+
+
 def reference_arm(args, rank, world):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    res = run_reference_sample(args.size, args.warmup + args.steps, args.ref_cycles, threads)
+    res = cpu_sample(args.cpu_ref, args.size, args.warmup + args.steps, args.ref_cycles, threads)
     timed = res["sample_s"][args.warmup:]
     cells = res["active_domain_cells"]
     cycles = res["cycles_per_sample"] * len(timed)
     value = cells * cycles / sum(timed)
     n = args.size
+    path = ("the reference's OpenMP CPU path" if res["kind"] == "reference"
+            else "the oracle's serial restatement of the reference")
+    init = "the reference's own initialisation" if res["kind"] == "reference" else "the restatement's initialisation"
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * sum(timed) / len(timed), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64/f32 (reference mixed precision)", "data": "synthetic",
         "config": {"workload": f"directional solidification {n}^3, G=R=1e6, N=25, 1e14 m^-3 nuclei",
-                   "cells": cells, "step": f"{args.ref_cycles} CA cycles of the reference's OpenMP CPU path",
-                   "l2": "n/a (CPU)"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["threads"], "kind": "reference",
+                   "cells": cells, "step": f"{args.ref_cycles} CA cycles of {path}", "l2": "n/a (CPU)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": res["threads"], "kind": res["kind"],
                          "sample": f"CA cycles {args.warmup * args.ref_cycles + 1}-{res['cycles']} of the {n}^3 "
-                                   f"solve after the reference's own initialisation ({res['init_s']:.1f} s)"},
+                                   f"solve after {init} ({res['init_s']:.1f} s)"},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -337,11 +393,12 @@ def b200_arm(args, rank, world, local):
         if world == 1 and not args.no_cpu_baseline:
             try:
                 threads = os.cpu_count() or 1
-                res = run_reference_sample(n, 1, args.ref_cycles, threads)
+                res = cpu_sample(args.cpu_ref, n, 1, args.ref_cycles, threads)
                 v = res["active_domain_cells"] * res["cycles_per_sample"] / res["sample_s"][0]
-                line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": res["threads"], "kind": "reference",
-                                        "sample": f"CA cycles 1-{res['cycles']} of the same {n}^3 solve, reference "
-                                                  f"OpenMP CPU path after its own initialisation"}
+                what = ("reference OpenMP CPU path after its own initialisation" if res["kind"] == "reference"
+                        else "oracle's serial restatement of the reference")
+                line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": res["threads"], "kind": res["kind"],
+                                        "sample": f"CA cycles 1-{res['cycles']} of the same {n}^3 solve, {what}"}
             except Exception as e:  # the baseline is reported, never required
                 line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                         "sample": f"unavailable: {e}"}
@@ -496,6 +553,9 @@ def main():
     ap.add_argument("--profile-at", type=int, default=6000)
     ap.add_argument("--profile-cycles", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-ref", default="auto", choices=["auto", "reference", "port"],
+                    help="CPU path timed by --impl reference and the cpu_baseline: the reference's own OpenMP "
+                         "build (oracle/_ref), the oracle's serial restatement, or the former when built")
     ap.add_argument("--workload", default="plain", choices=["plain", "batch", "serve"],
                     help="plain: the 512^3 headline; batch / serve: the process-map workloads (1 GPU)")
     ap.add_argument("--domains", type=int, default=256)
