@@ -1,12 +1,31 @@
 """Shared helpers of the parity tests (test infrastructure)."""
 import os
+import subprocess
 import tempfile
 
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
 GOLDEN = os.path.join(HERE, "golden")
 INPUTS = os.path.join(GOLDEN, "inputs")
+REF_SERIAL = os.path.join(ROOT, "oracle", "_ref", "ExaCA-ref-serial")
+
+
+def reference_error(path):
+    """The exception message of the reference (compiled against single-rank shims in oracle/_ref)
+    on this input file, run from the file's folder: '' when it initialises and runs to the end, None
+    when the reference was not built here."""
+    if not os.path.exists(REF_SERIAL):
+        return None
+    r = subprocess.run([REF_SERIAL, os.path.basename(path)], cwd=os.path.dirname(path), capture_output=True,
+                       text=True, timeout=600,
+                       env=dict(os.environ, EXACA_DATA_DIR=os.path.join(ROOT, "exaca_b200", "data")))
+    for ln in (r.stdout + r.stderr).splitlines():
+        if "what():" in ln:
+            return ln.split("what():", 1)[1].strip()
+    assert r.returncode == 0, r.stderr[-2000:]
+    return ""
 
 
 def golden_cases():

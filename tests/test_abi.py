@@ -8,7 +8,7 @@ import re
 import numpy as np
 import pytest
 
-from helpers import input_path
+from helpers import input_path, reference_error
 
 import exaca_b200 as ex
 
@@ -93,6 +93,9 @@ def test_malformed_inputs(lib, tmp_path, lines, code, msg):
     assert e.value.code == code
     if msg:
         assert msg in str(e.value)
+    # the reference itself (where built here) stops on the same file with the same message
+    ref = reference_error(str(path))
+    assert ref is None or (ref and ref in str(e.value)), (ref, str(e.value))
 
 
 def test_multilayer_problem_and_layer_limit(lib, tmp_path):

@@ -5,32 +5,15 @@ limit on distinct UndercoolingChange values (one growth table each). Each case i
 golden problem with one change. Where the reference compiled against single-rank shims is present
 (oracle/_ref), it runs on the same files and must raise the same message (or none)."""
 import os
-import subprocess
 
 import pytest
+from helpers import reference_error
 
 import exaca_b200 as ex
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 INPUTS = os.path.join(ROOT, "tests", "golden", "inputs")
 TRACK = os.path.join(INPUTS, "temperatures", "track_h2.csv")
-REF = os.path.join(ROOT, "oracle", "_ref", "ExaCA-ref-serial")
-
-
-def reference_error(path):
-    """The reference's exception message on this input ('' when it initialises and runs), or None
-    when the reference was not built here."""
-    if not os.path.exists(REF):
-        return None
-    r = subprocess.run([REF, os.path.basename(path)], cwd=os.path.dirname(path), capture_output=True, text=True,
-                       timeout=600, env=dict(os.environ, EXACA_DATA_DIR=os.path.join(ROOT, "exaca_b200", "data")))
-    for ln in (r.stdout + r.stderr).splitlines():
-        if "what():" in ln:
-            return ln.split("what():", 1)[1].strip()
-    assert r.returncode == 0, r.stderr[-2000:]
-    return ""
-
-
 def r_case(tmp_path, header=None, first_line=None, mesh=None, rate=None):
     """RTrackH2 with its temperature file copied to tmp_path and changed as asked."""
     rows = open(TRACK).read().splitlines()
