@@ -1,9 +1,10 @@
-"""Edge inputs without stored fixtures (no GPU). The reference itself (its unmodified sources
-compiled here against single-rank shims, oracle/_ref) runs on each; this solver's host
-initialisation must reproduce its post-init fields and the CPU restatement oracle its final
-GrainID / CellType and cycle, bit for bit. Cases: no substrate seeds (growth from nuclei only),
-every surface site active, a domain of 3 cells a side, a flat uneven box, one small spot, and a
-spot melt with dense nucleation. Skipped where the reference was not built."""
+"""Edge inputs without stored fixtures. The reference itself (its unmodified sources compiled here
+against single-rank shims, oracle/_ref) runs on each; this solver's host initialisation must
+reproduce its post-init fields and the CPU restatement oracle its final GrainID / CellType and
+cycle, bit for bit (no GPU; skipped where the reference was not built). On a GPU the CUDA path
+must then equal the restatement on the same inputs. Cases: no substrate seeds (growth from nuclei
+only), every surface site active, a domain of 3 cells a side, a flat uneven box, one small spot,
+and a spot melt with dense nucleation."""
 import os
 import re
 import shutil
@@ -99,3 +100,28 @@ def test_edge_input_matches_reference(lib, case):
         assert np.array_equal(fo["cell_type"].astype(np.int8), ref_ct)
     finally:
         shutil.rmtree(work, ignore_errors=True)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("case", sorted(CASES))
+def test_edge_input_gpu_matches_restatement(lib, tmp_path, case):
+    # the restatement is pinned to the reference on these inputs by the test above
+    base, changes = CASES[case]
+    inp = str(tmp_path / "input.txt")
+    write_variant(base, changes, inp)
+    o = Oracle(inp)
+    cycle = o.run()
+    f = o.fields()
+    p = ex.Problem.from_file(inp)
+    pool = ex.Pool(0, list_capacity=p.geometry.active_size)
+    try:
+        slot = pool.admit(p, device_check=False)
+        assert pool.run_plain(slot) == cycle
+        gid, ct = pool.copy_out(slot)
+        dl, _, _ = pool.copy_octahedra(slot)
+        assert pool.status(slot).error == 0
+    finally:
+        pool.close()
+    assert np.array_equal(ct, f["cell_type"]), f"{np.sum(ct != f['cell_type'])} CellType differ"
+    assert np.array_equal(gid, f["grain_id"]), f"{np.sum(gid != f['grain_id'])} GrainID differ"
+    assert np.array_equal(dl, f["dl"]), f"{np.sum(dl != f['dl'])} DiagonalLength differ"
