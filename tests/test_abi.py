@@ -1,7 +1,6 @@
 """C ABI surface and host-side behaviour of the native library, without a GPU: every function the
 header declares is exported, problems are built and described on the host, and malformed inputs
 fail with the reference's messages (src/CAinitialize.cpp:36-229) as error codes, not exceptions."""
-import ctypes
 import os
 import re
 
