@@ -768,7 +768,7 @@ void nuclei_init(Problem &p, std::string &log) {
 // the plane CritTimeSteps, the substrate seeds and the nuclei come from the same random streams
 // in the same orders as the dense path above; the dense fields are made from them on the device at
 // admission (and by materialize_fields on the host).
-void init_directional_seeds(Problem &p, std::string &log) {
+void init_directional_seeds(Problem &p, std::string & /* log: type C adds no notes */) {
     Geometry &g = p.g;
     const InputConfig &c = p.cfg;
     g.zbound_low = 0;
