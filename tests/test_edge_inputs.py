@@ -4,7 +4,8 @@ reproduce its post-init fields and the CPU restatement oracle its final GrainID 
 cycle, bit for bit (no GPU; skipped where the reference was not built). On a GPU the CUDA path
 must then equal the restatement on the same inputs. Cases: no substrate seeds (growth from nuclei
 only), every surface site active, a domain of 3 cells a side, a flat uneven box, one small spot,
-and a spot melt with dense nucleation."""
+and a spot melt with dense nucleation; on the host only, spot melts of two and five layers and
+type-R problems with one file repeated over layers and with a one-cell layer offset."""
 import os
 import re
 import shutil
@@ -14,7 +15,7 @@ import tempfile
 
 import numpy as np
 import pytest
-from helpers import INPUTS, REF_SERIAL, to_whole
+from helpers import INPUTS, REF_SERIAL, resolve_temperature_path, to_whole
 from oracle_port import Oracle
 
 import exaca_b200 as ex
@@ -41,6 +42,17 @@ CASES = {
     "dense_nuclei_spot": ("SmallSpotMelt", {"Radii of spots": "10", "Offset between spot centers": "10",
                                             "Heterogeneous nucleation density": "20000"}),
 }
+# Several layers and temperature-file series, checked on the host only (the CUDA path's multilayer
+# and type-R parity runs on the stored fixtures and on seeded random problems against the oracle)
+LAYERED_CASES = {
+    "spot_two_layers": ("SpotMelt3Layers", {"Number of layers": "2", "Offset between layers": "3",
+                                            "Number of spots in x": "1", "Radii of spots": "7",
+                                            "Offset between spot centers": "7", "Substrate grain spacing": "4"}),
+    "spot_five_thin_layers": ("SpotMelt3Layers", {"Number of layers": "5", "Offset between layers": "2",
+                                                  "Heterogeneous nucleation density": "2000"}),
+    "r_one_file_two_layers": ("RTrackH2", {"Number of layers": "2", "Offset between layers": "3"}),
+    "r_layer_offset_one": ("RTwoFiles3Layers", {"Offset between layers": "1"}),
+}
 
 
 def write_variant(base, changes, path):
@@ -49,7 +61,7 @@ def write_variant(base, changes, path):
         for key, value in changes.items():
             if ln.startswith(key):
                 ln = ln[: ln.rfind(":") + 1] + " " + value
-        out.append(ln)
+        out.append(resolve_temperature_path(ln))
     open(path, "w").write("\n".join(out) + "\n")
 
 
@@ -71,9 +83,9 @@ def run_reference(inp, work):
 
 
 @pytest.mark.skipif(not os.path.exists(REF_SERIAL), reason="the reference was not built here (make -C oracle ref)")
-@pytest.mark.parametrize("case", sorted(CASES))
+@pytest.mark.parametrize("case", sorted(CASES) + sorted(LAYERED_CASES))
 def test_edge_input_matches_reference(lib, case):
-    base, changes = CASES[case]
+    base, changes = CASES.get(case) or LAYERED_CASES[case]
     work = tempfile.mkdtemp(prefix=f"edge_{case}_")
     try:
         inp = os.path.join(work, "input.txt")

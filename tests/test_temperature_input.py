@@ -1,6 +1,7 @@
 """Type-R input errors on the host (no GPU): the reference's messages for a temperature-file
 header with a wrong column (src/CAinitialize.cpp:149-175), the old header format (:763-775) and a
-temperature grid that is not a whole multiple of the cell size (:1140-1152), plus the solver's own
+temperature grid that is not a whole multiple of the cell size (:1140-1152) and a missing
+temperature file (:201-209), plus the solver's own
 limit on distinct UndercoolingChange values (one growth table each). Each case is the RTrackH2
 golden problem with one change. Where the reference compiled against single-rank shims is present
 (oracle/_ref), it runs on the same files and must raise the same message (or none)."""
@@ -89,3 +90,21 @@ def test_too_many_undercooling_values(lib, tmp_path):
     with pytest.raises(ex.ExacaError) as e:
         ex.Problem.from_file(path)
     assert e.value.code == -2 and "distinct UndercoolingChange values" in str(e.value)
+
+
+def test_missing_temperature_file(lib, tmp_path):
+    # one file in the series: its name carries no number, and only numbered files exist here
+    lines = []
+    for ln in open(os.path.join(INPUTS, "RTwoFiles3Layers.txt")).read().splitlines():
+        if ln.startswith("Number of temperature files"):
+            ln = "Number of temperature files: 1"
+        elif ln.startswith("Path to temperature file"):
+            ln = "Path to temperature file(s): " + os.path.join(INPUTS, "temperatures")
+        lines.append(ln)
+    path = tmp_path / "in.txt"
+    path.write_text("\n".join(lines) + "\n")
+    msg = "Could not locate/open Temperature file"
+    with pytest.raises(ex.ExacaError) as e:
+        ex.Problem.from_file(str(path))
+    assert e.value.code == -1 and msg in str(e.value)
+    assert reference_error(str(path)) in (None, msg)
