@@ -1,7 +1,7 @@
 """Edge inputs without stored fixtures. The reference itself (its unmodified sources compiled here
 against single-rank shims, oracle/_ref) runs on each; this solver's host initialisation must
-reproduce its post-init fields and the CPU restatement oracle its final GrainID / CellType and
-cycle, bit for bit (no GPU; skipped where the reference was not built). On a GPU the CUDA path
+reproduce its post-init fields, its output writer the reference's .vtk files from the reference's
+final GrainID, and the CPU restatement oracle its final GrainID / CellType and cycle, bit for bit (no GPU; skipped where the reference was not built). On a GPU the CUDA path
 must then equal the restatement on the same inputs. Cases: no substrate seeds (growth from nuclei
 only), every surface site active, a domain of 3 cells a side, a flat uneven box, one small spot,
 and a spot melt with dense nucleation; on the host only, spot melts of two and five layers and
@@ -66,7 +66,8 @@ def write_variant(base, changes, path):
 
 
 def run_reference(inp, work):
-    """Post-init fields (the reference's debug dump), final GrainID / CellType and final cycle."""
+    """Post-init fields (the reference's debug dump), final GrainID / CellType, final cycle and the
+    prefix of the output files it wrote."""
     dbg_inp = os.path.join(work, "debug_input.txt")
     make_golden.debug_variant(inp, dbg_inp, work)
     base = next(ln.split(":", 1)[1].strip() for ln in open(inp) if ln.startswith("Output file base name"))
@@ -79,7 +80,7 @@ def run_reference(inp, work):
     cycle = int(re.search(r"output written at cycle (\d+)", open(os.path.join(work, base + ".log")).read()).group(1))
     gid = np.fromfile(os.path.join(dump, "GrainID.bin"), np.int32)
     ct = np.fromfile(os.path.join(dump, "CellType.bin"), np.int32).astype(np.int8)
-    return dbg, gid, ct, cycle
+    return dbg, gid, ct, cycle, os.path.join(work, base)
 
 
 @pytest.mark.skipif(not os.path.exists(REF_SERIAL), reason="the reference was not built here (make -C oracle ref)")
@@ -90,7 +91,7 @@ def test_edge_input_matches_reference(lib, case):
     try:
         inp = os.path.join(work, "input.txt")
         write_variant(base, changes, inp)
-        dbg, ref_gid, ref_ct, ref_cycle = run_reference(inp, work)
+        dbg, ref_gid, ref_ct, ref_cycle, ref_prefix = run_reference(inp, work)
 
         # host initialisation of this solver
         p = ex.Problem.from_file(inp)
@@ -103,6 +104,13 @@ def test_edge_input_matches_reference(lib, case):
         gid = to_whole(f["grain_id"], shape)
         pending = gid == ex.VORONOI_PENDING  # type S baseplate grains are assigned on the device
         assert np.array_equal(gid[~pending], dbg["GrainID"].astype(np.int32)[~pending])
+
+        # output files written from the reference's final GrainID: the reference's bytes
+        ours = os.path.join(work, "ours")
+        p.write_outputs(ref_gid, ours)
+        for suffix in (".vtk", "_Misorientations.vtk"):
+            assert os.path.exists(ref_prefix + suffix)
+            assert open(ours + suffix, "rb").read() == open(ref_prefix + suffix, "rb").read(), suffix
 
         # the CPU restatement oracle, run to the end
         o = Oracle(inp)
