@@ -93,6 +93,8 @@ class CellFieldsT(ctypes.Structure):
 
 CENSUS_MAX_DOMAINS = 256
 STEP_CONFIGS = 8
+# device error flags (exaca_domain_status.error; include/exaca_b200.h EXACA_FLAG_*)
+FLAG_GROWTH_TABLE, FLAG_LIST_OVERFLOW, FLAG_BOUNDS, FLAG_BARRIER = 1, 2, 4, 8
 
 class GrainStatsT(ctypes.Structure):
     _fields_ = [("region_cells", ctypes.c_int64), ("melted_cells", ctypes.c_int64), ("n_grains", ctypes.c_int64),
@@ -132,6 +134,7 @@ SIGNATURES = {
     "exaca_pool_profile_cycles": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_pool_timed_step": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_pool_profile_persistent": ([_P, _I, ctypes.POINTER(ctypes.c_double)], _I),
+    "exaca_pool_check_bounded_wait": ([_P, ctypes.POINTER(ctypes.c_int)], _I),
     "exaca_pool_run_all": ([_P, _I, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)], _I),
     "exaca_pool_status_many": ([_P, _I, ctypes.POINTER(_I), ctypes.POINTER(DomainStatus)], _I),
     "exaca_pool_grain_stats": ([_P, _I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(GrainStatsT)], _I),
@@ -359,6 +362,13 @@ class Pool:
         t = (ctypes.c_double * 4)()
         _check(load_library().exaca_pool_profile_cycles(self._h, n_cycles, t))
         return {"k_step_begin": t[0], "k_grow": t[1], "k_claim": t[2], "k_capture_pass": t[3]}
+
+    def check_bounded_wait(self) -> int:
+        """The persistent kernel's grid-wide wait run where nothing can release it: returns the device
+        error flags it left (FLAG_BARRIER after its 1 s limit; they are cleared again)."""
+        f = ctypes.c_int()
+        _check(load_library().exaca_pool_check_bounded_wait(self._h, ctypes.byref(f)))
+        return int(f.value)
 
     def profile_persistent(self, n_cycles: int) -> dict:
         """step(n_cycles) with the persistent kernel's timeline on; per-cycle averages (us)."""

@@ -323,6 +323,12 @@ int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms)
     });
 }
 
+int exaca_pool_check_bounded_wait(exaca_pool *pool, int *flags) {
+    if (!pool || !flags)
+        return fail(EXACA_ERR_ARG, "bad argument");
+    return guarded([&] { *flags = pool->pool->check_bounded_wait(); });
+}
+
 int exaca_pool_profile_persistent(exaca_pool *pool, int n_cycles, double *us) {
     if (!pool || !us || n_cycles < 0)
         return fail(EXACA_ERR_ARG, "bad argument");

@@ -1513,6 +1513,15 @@ template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 2) k
     flush_stats(P, st);
 }
 
+// The bounded wait of the meeting point taken to its limit: a cooperative launch of two blocks in
+// which block 0 leaves without arriving, so block 1's wait can only end by its time limit (it sets
+// kErrBarrier and returns, and the context stays usable).
+__global__ void __launch_bounds__(kBlock) k_meet_probe(PoolState *P) {
+    if (blockIdx.x == 0)
+        return;
+    grid_meet(P, -1, [] {});
+}
+
 // Compiled launch shapes: {capture lanes, growth batch} for kLaneChoices x kBatchChoices.
 struct StepKernels {
     const void *cycles;
@@ -2384,6 +2393,24 @@ void Pool::sync_state() {
         CUDA_OK(cudaMemcpyAsync(host_desc_.data(), ddesc_, sizeof(DomainDesc) * host_desc_.size(),
                                 cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
+}
+
+int Pool::check_bounded_wait() {
+    CUDA_OK(cudaSetDevice(device_));
+    cudaStream_t st = S(stream_);
+    CUDA_OK(cudaMemsetAsync((char *)dstate_ + offsetof(PoolState, bar_count), 0, 2 * sizeof(unsigned int), st));
+    PoolState *ps = dstate_;
+    void *args[] = {&ps};
+    CUDA_OK(cudaLaunchCooperativeKernel((const void *)k_meet_probe, dim3(2), dim3(kBlock), args, 0, st));
+    launches_ += 1;
+    const int flags = pool_error();
+    // the pool carries on: no flag and a meeting point with no arrivals
+    const int zero = 0;
+    CUDA_OK(cudaMemcpyAsync((char *)dstate_ + offsetof(PoolState, error), &zero, sizeof(int), cudaMemcpyHostToDevice,
+                            st));
+    CUDA_OK(cudaMemsetAsync((char *)dstate_ + offsetof(PoolState, bar_count), 0, 2 * sizeof(unsigned int), st));
+    CUDA_OK(cudaStreamSynchronize(st));
+    return flags;
 }
 
 int Pool::pool_error() {

@@ -263,6 +263,9 @@ class Pool {
     long long liquid(int slot) const;
     void set_cycle(int slot, int cycle);
     int pool_error();
+    // Runs the persistent kernel's grid-wide wait where nothing can release it; returns the pool
+    // error flags it left (kErrBarrier after the 1 s limit) and clears them.
+    int check_bounded_wait();
 
   private:
     void ensure_growth(int slot, long long needed);

@@ -59,7 +59,7 @@ typedef struct {
     int cycle;          /* last executed CA cycle */
     int done;           /* 1 once the domain met the reference's termination test */
     int nn;             /* nucleation events so far */
-    int error;          /* device error flags (0 = none) */
+    int error;          /* device error flags (0 = none; EXACA_FLAG_*) */
     int64_t liquid;     /* liquid cells left (device-checked single-layer slots) */
     int layer;          /* current layer (layernumber, src/runCA.cpp:282) */
     int window_z_lo;    /* the layer's active window: z planes [window_z_lo, window_z_lo + window_nz) */
@@ -147,6 +147,16 @@ int exaca_pool_timed_step(exaca_pool *pool, int n_cycles, double *ms);
  * cycle and start of the next (run by the last block alone)}. Pass times count from the release of
  * the previous meeting point. */
 int exaca_pool_profile_persistent(exaca_pool *pool, int n_cycles, double *us);
+/* Device error flags, as exaca_domain_status.error reports them. */
+#define EXACA_FLAG_GROWTH_TABLE 1  /* undercooling count beyond the growth table */
+#define EXACA_FLAG_LIST_OVERFLOW 2 /* active list or claim queue full */
+#define EXACA_FLAG_BOUNDS 4        /* an index out of range */
+#define EXACA_FLAG_BARRIER 8       /* a grid-wide wait of the persistent kernel gave up after 1 s */
+/* Diagnostic, no counterpart in the reference: the persistent kernel's grid-wide wait run where
+ * nothing can release it (two blocks, one of which leaves without arriving). The wait ends by its
+ * 1 s limit; *flags receives the flags it left (EXACA_FLAG_BARRIER), which are then cleared, and
+ * the pool stays usable. */
+int exaca_pool_check_bounded_wait(exaca_pool *pool, int *flags);
 /* Waits for the device and reads one slot's state. */
 int exaca_pool_status(exaca_pool *pool, int slot, exaca_domain_status *st);
 /* exaca_pool_status for n_slots slots with one device read (request loops poll many domains). */
