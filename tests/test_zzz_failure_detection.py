@@ -1,7 +1,8 @@
 """Failure detection without a GPU fault: the persistent kernel's grid-wide wait, run where nothing
 can release it (one of two blocks leaves without arriving), ends by its 1 s limit with the barrier
 flag set instead of hanging; the host reads the flag, and the same pool then solves a golden case
-bit for bit (the context stays usable)."""
+bit for bit (the context stays usable). Admission beyond the pool's HBM budget is refused before
+anything is allocated."""
 import time
 
 import numpy as np
@@ -34,3 +35,15 @@ def test_bounded_wait_gives_up_and_the_pool_carries_on(lib):
     assert cycle == int(g["cycle"])
     assert np.array_equal(gid, g["final_grain_id"])
     assert np.array_equal(ct.astype(np.int8), g["final_cell_type"])
+
+
+def test_admission_beyond_the_budget_is_refused(lib):
+    p = ex.Problem.from_file(input_path("SmallDirS"))
+    pool = ex.Pool(0, budget_bytes=p.slot_bytes() - 1, list_capacity=p.geometry.active_size)
+    try:
+        with pytest.raises(ex.ExacaError) as e:
+            pool.admit(p, device_check=False)
+        assert e.value.code == -4 and "HBM budget" in str(e.value)
+        assert pool.bytes_in_use() == 0
+    finally:
+        pool.close()
