@@ -27,6 +27,7 @@
 // Arithmetic follows the reference's types and operation order; this file is compiled with
 // -fmad=false so no multiply-add is contracted, and sqrt/division are IEEE round-to-nearest.
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <chrono>
@@ -2081,7 +2082,16 @@ void Pool::ensure_growth(int slot, long long needed) {
                             sizeof(h.growth_len), cudaMemcpyHostToDevice, S(stream_)));
 }
 
+// Named range on the host timeline for profilers (NVTX; inert when no tool is attached).
+struct TraceRange {
+    explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange &) = delete;
+    TraceRange &operator=(const TraceRange &) = delete;
+};
+
 int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
+    TraceRange trace("exaca admit");
     CUDA_OK(cudaSetDevice(device_));
     const Problem &p = *pp;
     if (p.g.zbound_low != 0)
@@ -2285,6 +2295,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
 }
 
 void Pool::retire(int slot) {
+    TraceRange trace("exaca retire");
     CUDA_OK(cudaSetDevice(device_));
     SlotHost &s = slots_.at(slot);
     if (!s.used)
@@ -2360,6 +2371,7 @@ void Pool::build_graph() {
 }
 
 void Pool::step(int n) {
+    TraceRange trace("exaca step");
     if (n <= 0)
         return;
     cycles_launched_ += (unsigned long long)n;
@@ -2571,6 +2583,7 @@ int Pool::autotune(int trial_cycles, double *ms_per_cycle) {
 }
 
 long long Pool::run_all(int chunk, long long max_cycles) {
+    TraceRange trace("exaca run_all");
     if (chunk <= 0)
         throw std::invalid_argument("chunk must be positive");
     long long stepped = 0;
@@ -2655,6 +2668,7 @@ void Pool::set_cycle(int slot, int cycle) {
 }
 
 void Pool::next_layer(int slot, std::string &log) {
+    TraceRange trace("exaca next_layer");
     // src/runCA.cpp:344-405: DomainShiftAndResize, then LayerSetup on the moved window
     CUDA_OK(cudaSetDevice(device_));
     cudaStream_t st = S(stream_);
@@ -2754,6 +2768,7 @@ void Pool::copy_octahedra(int slot, float *dl, float *doc, float *cdl) {
 }
 
 void Pool::copy_out(int slot, int32_t *grain_id, int32_t *cell_type) {
+    TraceRange trace("exaca copy_out");
     if (!cell_type) {
         copy_out_raw(slot, grain_id, nullptr);
         return;
@@ -2778,6 +2793,7 @@ void Pool::copy_out(int slot, int32_t *grain_id, int32_t *cell_type) {
 }
 
 void Pool::copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type) {
+    TraceRange trace("exaca copy_out_concurrent");
     CUDA_OK(cudaSetDevice(device_));
     const SlotHost &s = slots_.at(slot);
     const DomainDesc &d = host_desc_.at(slot);
@@ -2808,6 +2824,7 @@ void Pool::copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type) 
 }
 
 int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_s) {
+    TraceRange trace("exaca run_plain");
     // src/runCA.cpp:282-411: the layer loop, each layer's cycles until no liquid of the layer is left
     const Problem &p = *slots_.at(slot).problem;
     const bool type_r = p.cfg.simulation_type == "R";
