@@ -211,6 +211,7 @@ struct Serial {
 using DefaultExecutionSpace = Serial;
 
 inline void initialize(int &, char **) {}
+inline void initialize() {}
 inline void finalize() {}
 inline void fence() {}
 
