@@ -33,9 +33,15 @@ def request_stream(n_requests: int = 200, rate: float = 200.0, seed: int = 4, si
 
 
 def serve(requests: list, device: int = 0, budget_bytes: int = 150 * 10**9, chunk_cycles: int = 250,
-          list_capacity: int = 1 << 27, init_threads: int | None = None, keep_results: bool = False) -> dict:
+          list_capacity: int = 1 << 27, init_threads: int | None = None, keep_results: bool = False,
+          deadline_s: float | None = None, pool_factory=Pool) -> dict:
     """Runs the request loop in real time and returns per-request latencies (s, arrival to result
-    on the host), completion order and, with keep_results, each GrainID / CellType / final cycle."""
+    on the host), completion order and, with keep_results, each GrainID / CellType / final cycle.
+
+    deadline_s: a request whose result is not on the host that many seconds after its arrival is
+    given up (its slot retired while the others run on, or never admitted); it is listed in
+    `timed_out` and has no latency. pool_factory(device, budget_bytes=, list_capacity=) makes the
+    pool (exaca_b200.Pool; tests pass a host-only stand-in)."""
     init_threads = init_threads or os.cpu_count() or 1
     n = len(requests)
     ready: queue.Queue = queue.Queue()
@@ -56,12 +62,13 @@ def serve(requests: list, device: int = 0, budget_bytes: int = 150 * 10**9, chun
     for k in range(n):
         workers.submit(init_one, k)
 
-    pool = Pool(device, budget_bytes=budget_bytes, list_capacity=list_capacity)
+    pool = pool_factory(device, budget_bytes=budget_bytes, list_capacity=list_capacity)
     latency = [None] * n
     results = [None] * n
     waiting = []  # initialised, not admitted yet (arrival order)
     resident = {}  # slot -> request index
     finished = []  # (slot, request index, final cycle) ended at the last status read
+    timed_out = []
     done_count = 0
     steps = 0
     try:
@@ -76,6 +83,18 @@ def serve(requests: list, device: int = 0, budget_bytes: int = 150 * 10**9, chun
             except queue.Empty:
                 pass
             waiting.sort(key=lambda kp: requests[kp[0]][0])
+            if deadline_s is not None:
+                # give up requests past their deadline: waiting ones are dropped, resident ones
+                # retired (those already ended on the device complete below)
+                now = time.perf_counter() - t_start
+                late = [kp for kp in waiting if now - requests[kp[0]][0] > deadline_s]
+                waiting = [kp for kp in waiting if now - requests[kp[0]][0] <= deadline_s]
+                for slot in [sl for sl, k in resident.items() if now - requests[k][0] > deadline_s]:
+                    pool.retire(slot)
+                    late.append((resident.pop(slot), None))
+                for k, _ in late:
+                    timed_out.append(k)
+                    done_count += 1
             # admit in arrival order while the budget allows
             still = []
             for k, prob in waiting:
@@ -115,9 +134,11 @@ def serve(requests: list, device: int = 0, budget_bytes: int = 150 * 10**9, chun
     finally:
         workers.shutdown(wait=True)
         pool.close()
-    lat = np.array(latency)
-    return dict(latency=latency, results=results, elapsed=elapsed, solves_per_s=n / elapsed, steps=steps,
-                p50=float(np.percentile(lat, 50)), p99=float(np.percentile(lat, 99)))
+    lat = np.array([x for x in latency if x is not None], dtype=np.float64)
+    return dict(latency=latency, results=results, elapsed=elapsed, solves_per_s=len(lat) / elapsed, steps=steps,
+                timed_out=sorted(timed_out),
+                p50=float(np.percentile(lat, 50)) if len(lat) else float("nan"),
+                p99=float(np.percentile(lat, 99)) if len(lat) else float("nan"))
 
 
 def sequential_plain(requests: list, device: int = 0) -> dict:
