@@ -12,8 +12,16 @@ metric: cell-updates/s = active-window cells x CA cycles executed / solve time (
 per-cycle sweep size times cycles). `value` is timed with CUDA events around each solve with the
 initial state already resident in HBM; `e2e` times the same K solves through the C ABI, each
 with its admission (upload of the seeds the cell fields are made from on the device, the fields'
-construction), the solve and the GrainID/CellType download into pinned host buffers. The state (~20 GB) is larger
-than L2 and is rebuilt between steps.
+construction), the solve and the GrainID/CellType download into pinned host buffers;
+`e2e.with_host_init` adds the host's parsing and initialisation of the input file to every step, as
+the drop-in executable runs it. The state (~20 GB) is larger than L2 and is rebuilt between steps.
+
+`parity` checks the timed solve itself: SHA-256 digests of the last e2e solve's GrainID and CellType
+against those pinned in tests/golden/DirS512.json (the oracle's restatement run to termination), and
+of a solve stopped after cycle 5000 against the unmodified reference at that cycle. `batch` and
+`serve` carry the process-map workloads (256 uneven domains in one pool; a Poisson request stream
+with continuous batching) against their plain one-solve-per-launch paths, measured in the same run
+(`--no-process-map` leaves them out; `--workload batch|serve` prints either alone).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--size S]
                     [--cpu-ref auto|reference|port]
@@ -105,6 +113,26 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def pinned_digests(n):
+    """SHA-256 digests of the n^3 solve pinned in tests/golden/DirS<n>.json (GrainID as int32 and
+    CellType as int8 over the whole cell array): at termination from the oracle's restatement, and
+    after 5000 cycles from the reference itself. None when no such file was generated."""
+    path = os.path.join(ROOT, "tests", "golden", f"DirS{n}.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        return json.load(f)
+
+
+def digests(grain_id, cell_type):
+    import hashlib
+
+    import numpy as np
+
+    return {"sha_grain_id": hashlib.sha256(np.ascontiguousarray(grain_id, dtype=np.int32).tobytes()).hexdigest(),
+            "sha_cell_type": hashlib.sha256(np.ascontiguousarray(cell_type).astype(np.int8).tobytes()).hexdigest()}
 
 
 class ClockSampler:
@@ -342,6 +370,55 @@ def b200_arm(args, rank, world, local):
     d2h = (se1["d2h_bytes"] - se0["d2h_bytes"]) // args.steps
     e2e_value = world * cells * c_e / e2e_s
 
+    # parity of the timed solve (untimed): the last e2e step's GrainID / CellType against the pinned
+    # digests of the same input, and a second solve stopped after the reference-pinned cycle
+    pins = pinned_digests(n)
+    parity = {"checked": False, "why": f"no tests/golden/DirS{n}.json for this size"}
+    if pins is not None:
+        last = digests(gid.numpy(), ct.numpy())
+        fin = pins.get("final", {})
+        slot = pool.admit(prob, device_check=False)
+        pool.step(pins["pin_cycle"])
+        g5, c5 = pool.copy_out(slot)
+        pool.retire(slot)
+        at_pin = digests(g5, c5)
+        del g5, c5
+        ref_pin = pins.get("cycle5000_reference", {})
+        parity = {
+            "checked": True,
+            "final_vs_restatement": bool(fin) and last == {k: fin[k] for k in last} and c_e == fin["cycle"] * args.steps,
+            "final_cycle": c_e // args.steps, "restatement_final_cycle": fin.get("cycle"),
+            f"cycle{pins['pin_cycle']}_vs_reference": bool(ref_pin) and at_pin == {k: ref_pin[k] for k in at_pin},
+            "what": "SHA-256 of GrainID (int32) and CellType (int8) over all cells of the last e2e solve, against "
+                    "the oracle's restatement run to termination; a further solve stopped after cycle "
+                    f"{pins['pin_cycle']}, against the unmodified reference (Serial order) at that cycle "
+                    "(tests/golden/make_dirs512.py)",
+        }
+        parity["ok"] = parity["final_vs_restatement"] and parity[f"cycle{pins['pin_cycle']}_vs_reference"]
+
+    # end to end as the drop-in runs it: the input file parsed and the problem initialised on the
+    # host (the reference's init), then admission, solve and copy-out, every step
+    with tempfile.TemporaryDirectory() as tmp:
+        inp = os.path.join(tmp, "bench.txt")
+        with open(inp, "w") as f:
+            f.write(input_file_text(n))
+        barrier()
+        full_s, c_f, init_f = 0.0, 0, 0.0
+        host_steps = min(args.steps, 3)  # ~1.3 s of host initialisation each at 512^3
+        for _ in range(host_steps):
+            t_f = time.perf_counter()
+            p_f = ex.Problem.from_file(inp)
+            init_f += time.perf_counter() - t_f
+            slot = pool.admit(p_f, device_check=False)
+            c_f += pool.run_plain(slot)
+            rc = lib.exaca_pool_copy_out(pool._h, slot, gid.data_ptr(), ct.data_ptr())
+            full_s += time.perf_counter() - t_f
+            if rc != 0:
+                raise RuntimeError(lib.exaca_last_error())
+            pool.retire(slot)
+            del p_f
+        full_s = max_over_ranks(full_s)
+
     # roofline of the persistent kernel (k_cycles, the only kernel of the timed solve apart from
     # the 1000-cycle census) on a bounded stretch of the solve: one launch, CUDA events around it
     slot = pool.admit(prob, device_check=False)
@@ -380,10 +457,18 @@ def b200_arm(args, rank, world, local):
                        "host_init_s": round(init_s, 2)},
             "clocks": clock_info,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-                    "seconds": e2e_s},
+                    "seconds": e2e_s,
+                    "with_host_init": {"value": world * cells * c_f / full_s, "unit": UNIT, "seconds": full_s,
+                                       "steps": host_steps, "host_init_s_per_step": init_f / host_steps,
+                                       "what": "input file parsed and problem initialised on the host every "
+                                               "step, then admission, solve and copy-out"}},
+            "parity": parity,
             "gpu_launches": launches,
             "roofline": {"bound": "hbm", "kernel": "k_cycles", "achieved": achieved, "peak": peak,
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "traffic_source": "not measured in this run: ncu DRAM bytes per cycle of a 1000-cycle "
+                                           "k_cycles launch (profiles/traffic_per_launch.txt) x the cycles of "
+                                           "this launch",
                          "algorithmic_bytes_per_launch": launch_bytes, "launch_ms": launch_ms,
                          "sample": f"one launch over cycles {args.profile_at + 1}-{args.profile_at + args.profile_cycles}",
                          "pass_bytes_per_launch": pass_bytes,
@@ -392,18 +477,32 @@ def b200_arm(args, rank, world, local):
         }
         if world == 1 and not args.no_cpu_baseline:
             try:
+                # the reference arm's cycle window at the same --steps / --warmup: `warmup` untimed samples
+                # of ref_cycles cycles after initialisation, then `steps` timed ones
                 threads = os.cpu_count() or 1
-                res = cpu_sample(args.cpu_ref, n, 1, args.ref_cycles, threads)
-                v = res["active_domain_cells"] * res["cycles_per_sample"] / res["sample_s"][0]
+                res = cpu_sample(args.cpu_ref, n, args.warmup + args.steps, args.ref_cycles, threads)
+                timed = res["sample_s"][args.warmup:]
+                v = res["active_domain_cells"] * res["cycles_per_sample"] * len(timed) / sum(timed)
                 what = ("reference OpenMP CPU path after its own initialisation" if res["kind"] == "reference"
                         else "oracle's serial restatement of the reference")
+                first = args.warmup * args.ref_cycles + 1
                 line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": res["threads"], "kind": res["kind"],
-                                        "sample": f"CA cycles 1-{res['cycles']} of the same {n}^3 solve, {what}"}
+                                        "sample": f"CA cycles {first}-{res['cycles']} of the same {n}^3 solve "
+                                                  f"(cycles 1-{first - 1} untimed), {what}"}
             except Exception as e:  # the baseline is reported, never required
                 line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": None, "kind": "reference",
                                         "sample": f"unavailable: {e}"}
-        print(json.dumps(line), flush=True)
     pool.close()
+    # the process-map workloads (batched and served solves/s against their plain paths) under the
+    # same clock, as objects of the same line
+    if not args.no_process_map:
+        b = measure_batch(args, rank, world, local, dist, 1, 1)
+        sv = measure_serve(args, rank, world, local, dist, 1, 1)
+        if rank == 0:
+            line["batch"] = b
+            line["serve"] = sv
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
@@ -433,26 +532,26 @@ def _max_over_ranks(dist, x):
     return float(t.item())
 
 
-def batch_arm(args, rank, world, local):
+def measure_batch(args, rank, world, local, dist, steps, warmup):
     """Batched process map (256 uneven directional domains, every domain bit-exact with its own plain
-    run): batched solves/s against the plain one-domain-at-a-time path on a seeded sample. With N
-    GPUs the map is split by HBM footprint (greedy bin-packing, no per-cycle exchange) and the
-    time is the slowest rank's."""
+    run): batched solves/s against the plain one-domain-at-a-time path on a seeded sample. Host
+    initialisation is excluded from both arms (every problem is built before either clock starts).
+    With N GPUs the map is split by HBM footprint (greedy bin-packing, no per-cycle exchange) and
+    the time is the slowest rank's. Returns the measurement on rank 0, None elsewhere."""
     import numpy as np
 
     from exaca_b200 import batch
 
-    dist = _dist_setup(world, local)
     all_params = batch.process_map(args.domains, seed=3)
     mine = batch.partition([batch.footprint(p) for p in all_params], world)[rank]
     params = [all_params[i] for i in mine]
     t0 = time.perf_counter()
     probs = batch.build_problems(params)
     init_s = time.perf_counter() - t0
-    for w in range(args.warmup):
+    for _ in range(warmup):
         batch.solve_batch(probs[:8], device=local, config=0)
-    times, tuned = [], None
-    for _ in range(args.steps):
+    times, tuned, res = [], None, None
+    for _ in range(steps):
         if dist is not None:
             dist.barrier()
         res = batch.solve_batch(probs, device=local, autotune_cycles=50)
@@ -468,77 +567,102 @@ def batch_arm(args, rank, world, local):
         plain = len(sample) / sum(pl["seconds"])
     if dist is not None:
         dist.barrier()
-        dist.destroy_process_group()
     if rank != 0:
-        return
+        return None
     value = len(all_params) / min(times)
-    line = {
-        "metric": "batched solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 1e3 * min(times), "higher_is_better": True, "scaling": "strong",
-        "vs_baseline": None, "dtype": "f64/f32 (reference mixed precision), int32/int8",
-        "data": "synthetic (seeded process map)",
-        "config": {"workload": f"batched process map, {len(all_params)} directional domains, sides 32-128 per axis, "
-                               "G 1e5-5e6 K/m, R 1e4-1e6 K/s, nucleation 1e12-1e15 m^-3 (log-uniform)",
-                   "rank0_cells": int(sum(p.geometry.active_size for p in probs)), "rank0_host_init_s": round(init_s, 2),
-                   "parallelism": f"{world} GPU(s), domains split by footprint",
-                   "step": "admit all, autotune, step until every domain terminated, copy out all"},
+    return {
+        "metric": "batched solves/s", "value": value, "unit": "solves/s", "steps": steps, "warmup": warmup,
+        "ms_per_step": 1e3 * min(times), "scaling": "strong",
+        "workload": f"batched process map, {len(all_params)} directional domains, sides 32-128 per axis, "
+                    "G 1e5-5e6 K/m, R 1e4-1e6 K/s, nucleation 1e12-1e15 m^-3 (log-uniform)",
+        "rank0_cells": int(sum(p.geometry.active_size for p in probs)), "rank0_host_init_s": round(init_s, 2),
+        "parallelism": f"{world} GPU(s), domains split by footprint",
+        "step": "admit all, autotune, step until every domain terminated, copy out all",
+        "host_init": "excluded from both arms",
         "plain_solves_per_s": plain, "speedup_vs_plain": value / plain,
         "plain_sample": f"{len(sample)} seeded domains of rank 0 solved one at a time on one GPU (admit, run, copy out)",
         "sample_bit_exact": bool(exact), "autotune": {"config": tuned[0], "ms_per_cycle": tuned[1]},
         "cycles": {"max": int(max(res["cycle"])), "median": float(np.median(res["cycle"]))},
         "seconds": res["seconds"],
     }
-    print(json.dumps(line), flush=True)
 
 
-def serve_arm(args, rank, world, local):
+def measure_serve(args, rank, world, local, dist, steps, warmup):
     """Served process-map queries: Poisson arrivals (200/s) admitted under a 150 GB HBM budget per
-    GPU and stepped together; solves/s and p50/p99 latency against sequential plain launches. With
-    N GPUs requests are routed by footprint (greedy bin-packing of the stream, no per-cycle
-    exchange); solves/s uses the slowest rank's wall time, latency percentiles all requests."""
+    GPU and stepped together; solves/s and p50/p99 latency against sequential plain launches of the
+    first requests. Host initialisation is included in both arms (a served request is initialised
+    when it arrives; a plain launch initialises, admits, runs and copies out). The plain sample's
+    results must equal the served ones. With N GPUs requests are routed by footprint (greedy
+    bin-packing of the stream, no per-cycle exchange); solves/s uses the slowest rank's wall time,
+    latency percentiles all requests. Returns the measurement on rank 0, None elsewhere."""
     import numpy as np
 
     from exaca_b200 import batch, serve
 
-    dist = _dist_setup(world, local)
     all_reqs = serve.request_stream(args.requests, rate=200.0, seed=4)
     mine = batch.partition([batch.footprint(p) for _, p in all_reqs], world)[rank]
     reqs = [all_reqs[i] for i in mine]
-    for w in range(args.warmup):
+    n_plain = min(args.plain_sample, len(reqs))
+    for w in range(warmup):
         serve.serve(serve.request_stream(8, rate=200.0, seed=100 + w, side=(24, 48)), device=local)
     runs = []
-    for _ in range(args.steps):
+    for _ in range(steps):
         if dist is not None:
             dist.barrier()
-        runs.append(serve.serve(reqs, device=local))
+        runs.append(serve.serve(reqs, device=local, keep_results=set(range(n_plain)) if rank == 0 else False))
     best = max(runs, key=lambda r: r["solves_per_s"])
     elapsed = _max_over_ranks(dist, best["elapsed"])
-    lat = list(best["latency"])
+    lat = [x for x in best["latency"] if x is not None]
     if dist is not None:
         gathered = [None] * world
         dist.all_gather_object(gathered, lat)
         lat = [x for part in gathered for x in part]
-    pl = serve.sequential_plain(reqs[:args.plain_sample], device=local) if rank == 0 else None
+    pl, exact = None, None
+    if rank == 0:
+        pl = serve.sequential_plain(reqs[:n_plain], device=local)
+        exact = all(r is not None and q[2] == r[2] and np.array_equal(q[0], r[0]) and np.array_equal(q[1], r[1])
+                    for q, r in zip(pl["results"], best["results"][:n_plain]))
     if dist is not None:
         dist.barrier()
-        dist.destroy_process_group()
     if rank != 0:
-        return
+        return None
     value = len(all_reqs) / elapsed
-    line = {
-        "metric": "served solves/s", "value": value, "unit": "solves/s", "n_gpus": world,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed, "higher_is_better": True,
-        "scaling": "strong", "vs_baseline": None, "dtype": "f64/f32 (reference mixed precision), int32/int8",
-        "data": "synthetic (seeded Poisson request stream)",
-        "config": {"workload": f"served process-map queries, {len(all_reqs)} requests, Poisson 200/s, sides 48-256 "
-                               "per axis, G/R/nucleation as the batched map, 150 GB HBM budget per GPU",
-                   "parallelism": f"{world} GPU(s), requests routed by footprint",
-                   "step": "real-time request loop until every request's result is on the host"},
+    return {
+        "metric": "served solves/s", "value": value, "unit": "solves/s", "steps": steps, "warmup": warmup,
+        "ms_per_step": 1e3 * elapsed, "scaling": "strong",
+        "workload": f"served process-map queries, {len(all_reqs)} requests, Poisson 200/s, sides 48-256 per axis, "
+                    "G/R/nucleation as the batched map, 150 GB HBM budget per GPU",
+        "parallelism": f"{world} GPU(s), requests routed by footprint",
+        "step": "real-time request loop until every request's result is on the host",
+        "host_init": "included in both arms",
         "latency_s": {"p50": float(np.percentile(lat, 50)), "p99": float(np.percentile(lat, 99))},
+        "timed_out": len(best["timed_out"]),
         "plain_solves_per_s": pl["solves_per_s"], "speedup_vs_plain": value / pl["solves_per_s"],
         "plain_sample": f"first {len(pl['seconds'])} requests of rank 0 launched one after the other on one GPU "
                         "(init, admit, run, copy out)",
+        "sample_bit_exact": bool(exact),
     }
+
+
+def workload_arm(args, rank, world, local):
+    """`--workload batch|serve`: one JSON line for the process-map workload alone."""
+    dist = _dist_setup(world, local)
+    measure = measure_batch if args.workload == "batch" else measure_serve
+    m = measure(args, rank, world, local, dist, args.steps, args.warmup)
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {
+        "metric": m.pop("metric"), "value": m.pop("value"), "unit": m.pop("unit"), "n_gpus": world,
+        "steps": m.pop("steps"), "warmup": m.pop("warmup"), "ms_per_step": m.pop("ms_per_step"),
+        "higher_is_better": True, "scaling": m.pop("scaling"), "vs_baseline": None,
+        "dtype": "f64/f32 (reference mixed precision), int32/int8",
+        "data": "synthetic (seeded process map)" if args.workload == "batch" else
+                "synthetic (seeded Poisson request stream)",
+        "config": {"workload": m.pop("workload"), "parallelism": m.pop("parallelism"), "step": m.pop("step")},
+    }
+    line.update(m)
     print(json.dumps(line), flush=True)
 
 
@@ -549,10 +673,12 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--size", type=int, default=512)
-    ap.add_argument("--ref-cycles", type=int, default=40, help="CA cycles per reference sample")
+    ap.add_argument("--ref-cycles", type=int, default=20, help="CA cycles per reference sample")
     ap.add_argument("--profile-at", type=int, default=6000)
     ap.add_argument("--profile-cycles", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-process-map", action="store_true",
+                    help="plain workload without the batched / served process-map objects")
     ap.add_argument("--cpu-ref", default="auto", choices=["auto", "reference", "port"],
                     help="CPU path timed by --impl reference and the cpu_baseline: the reference's own OpenMP "
                          "build (oracle/_ref), the oracle's serial restatement, or the former when built")
@@ -565,10 +691,8 @@ def main():
     rank, world, local = dist_env()
     if args.impl == "reference":
         reference_arm(args, rank, world)
-    elif args.workload == "batch":
-        batch_arm(args, rank, world, local)
-    elif args.workload == "serve":
-        serve_arm(args, rank, world, local)
+    elif args.workload in ("batch", "serve"):
+        workload_arm(args, rank, world, local)
     else:
         b200_arm(args, rank, world, local)
 

@@ -87,7 +87,7 @@ class CellFieldsT(ctypes.Structure):
     _fields_ = [
         ("cell_type", ctypes.c_void_p), ("layer_id", ctypes.c_void_p), ("crit_time_step", ctypes.c_void_p),
         ("domain_size", ctypes.c_int64), ("active_size", ctypes.c_int64), ("cycle", ctypes.c_int32),
-        ("reserved", ctypes.c_int32),
+        ("layer", ctypes.c_int32), ("window_start", ctypes.c_int64),
     ]
 
 
@@ -123,6 +123,7 @@ SIGNATURES = {
     "exaca_pool_census": ([_P, _I, ctypes.POINTER(CensusT)], _I),
     "exaca_pool_stats": ([_P, ctypes.POINTER(PoolStatsT)], _I),
     "exaca_pool_run_plain": ([_P, _I, _I, ctypes.POINTER(_I)], _I),
+    "exaca_pool_next_layer": ([_P, _I, _I], _I),
     "exaca_pool_copy_out": ([_P, _I, _P, _P], _I),
     "exaca_pool_copy_out_concurrent": ([_P, _I, _P, _P], _I),
     "exaca_pool_copy_octahedra": ([_P, _I, _P, _P, _P], _I),
@@ -180,13 +181,14 @@ def census_cells(device: int, domains: list, stream: int = 0) -> list:
     """exaca_census_cells: IntermediateOutputAndCheck's census (src/CAupdate.cpp:738-808) of cell
     fields already in device memory, without allocating device memory. Each domain is a dict with
     the device addresses (ints) "cell_type" (int8), "layer_id" (int8), "crit_time_step" (int32) and
-    "domain_size", "active_size", "cycle"; at most CENSUS_MAX_DOMAINS per call. `stream` is a
-    cudaStream_t handle (0: the legacy default stream); the call waits for it."""
+    "domain_size", "active_size", "cycle", and optionally "layer" (the current layer, default 0) and
+    "window_start" (first cell of the active window, default 0); at most CENSUS_MAX_DOMAINS per
+    call. `stream` is a cudaStream_t handle (0: the legacy default stream); the call waits for it."""
     n = len(domains)
     arr = (CellFieldsT * max(n, 1))()
     for i, d in enumerate(domains):
         arr[i] = CellFieldsT(d["cell_type"], d["layer_id"], d["crit_time_step"], d["domain_size"],
-                             d["active_size"], d["cycle"], 0)
+                             d["active_size"], d["cycle"], d.get("layer", 0), d.get("window_start", 0))
     out = (CensusT * max(n, 1))()
     _check(load_library().exaca_census_cells(device, ctypes.c_void_p(stream), arr, n, out))
     return [{k: getattr(out[i], k) for k, _ in CensusT._fields_} for i in range(n)]
@@ -324,6 +326,10 @@ class Pool:
         c = ctypes.c_int()
         _check(load_library().exaca_pool_run_plain(self._h, slot, int(verbose), ctypes.byref(c)))
         return c.value
+
+    def next_layer(self, slot: int, verbose: bool = False) -> None:
+        """DomainShiftAndResize + LayerSetup of a multilayer slot (src/runCA.cpp:344-390)."""
+        _check(load_library().exaca_pool_next_layer(self._h, slot, int(verbose)))
 
     def copy_out(self, slot: int):
         n = self._problems[slot].geometry.domain_size

@@ -399,8 +399,10 @@ int exaca_census_cells(int device, void *stream, const exaca_cell_fields *domain
         return fail(EXACA_ERR_ARG, "null domains or out");
     for (int i = 0; i < n_domains; i++) {
         const exaca_cell_fields &d = domains[i];
-        if (d.domain_size < 0 || d.active_size < 0 || d.active_size > d.domain_size)
-            return fail(EXACA_ERR_ARG, "domain " + std::to_string(i) + ": bad domain_size / active_size");
+        if (d.domain_size < 0 || d.active_size < 0 || d.window_start < 0 ||
+            d.window_start > d.domain_size - d.active_size)
+            return fail(EXACA_ERR_ARG,
+                        "domain " + std::to_string(i) + ": bad domain_size / active_size / window_start");
         if (d.domain_size > 0 && (!d.cell_type || !d.layer_id || !d.crit_time_step))
             return fail(EXACA_ERR_ARG, "domain " + std::to_string(i) + ": null field pointer");
     }
@@ -420,6 +422,20 @@ int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cyc
             emit(log);
         if (final_cycle)
             *final_cycle = c;
+    });
+}
+
+int exaca_pool_next_layer(exaca_pool *pool, int slot, int verbose) {
+    if (!pool || !pool->pool->slot_used(slot))
+        return fail(EXACA_ERR_ARG, "bad slot");
+    const exaca::DomainDesc &d = pool->pool->state(slot);
+    if (d.layer_no + 1 >= d.n_layers)
+        return fail(EXACA_ERR_ARG, "slot " + std::to_string(slot) + " is in its last layer");
+    return guarded([&] {
+        std::string log;
+        pool->pool->next_layer(slot, log);
+        if (verbose)
+            emit(log);
     });
 }
 

@@ -8,8 +8,8 @@
 // reads a pool slot; this variant reads any caller arrays and keeps its working data in the
 // fixed file-scope array below instead.
 //
-// Scratch: kScratchBytes = 24 KiB, for at most kMaxDomains = 256 domains per call. The first
-// 256 * 48 bytes hold the copied domain descriptors, the next 256 * 48 bytes one accumulator of six
+// Scratch: kScratchBytes = 26 KiB, for at most kMaxDomains = 256 domains per call. The first
+// 256 * 56 bytes hold the copied domain descriptors, the next 256 * 48 bytes one accumulator of six
 // 64-bit counters per domain. Every call on a device shares this array and it keeps what the last
 // call left in it: each call copies its descriptors in and clears its accumulators to zero before
 // the kernel runs. Two calls whose work overlapped on the device would race on the array, so a
@@ -36,33 +36,36 @@ constexpr size_t kScratchBytes = kAccOffset + kMaxDomains * kAccWords * sizeof(u
 constexpr int kMaxDevices = 64;
 constexpr int kThreads = 256;
 
-static_assert(kDescBytes == 48, "exaca_cell_fields is 48 bytes on LP64");
+static_assert(kDescBytes == 56, "exaca_cell_fields is 56 bytes on LP64");
 static_assert(sizeof(exaca_census) == kAccWords * sizeof(unsigned long long), "exaca_census is six counters");
-static_assert(kScratchBytes == 24576, "24 KiB scratch");
+static_assert(kScratchBytes == 26624, "26 KiB scratch");
 
 static __device__ __align__(256) unsigned char g_census_scratch[kScratchBytes];
 
 // One accumulator per domain: superheated, undercooled, active, solid, remaining, and the bitwise
-// complement of the minimum CritTimeStep of liquid cells in the active window (so that all six
-// start at zero; zero means "no such cell" = ULLONG_MAX once complemented back).
+// complement of the minimum CritTimeStep of the layer's liquid cells in the active window (so that
+// all six start at zero; zero means "no such cell" = ULLONG_MAX once complemented back). Cells of
+// the current layer are classified (src/CAupdate.cpp:741-752), liquid cells of any other layer are
+// remaining (:754-757); the minimum is taken over the window only (:792-805).
 __global__ void __launch_bounds__(kThreads) k_census_cells(const exaca_cell_fields *cells, unsigned long long *acc) {
     const exaca_cell_fields d = cells[blockIdx.y];
     unsigned long long *out = acc + kAccWords * blockIdx.y;
     unsigned long long a[5] = {0, 0, 0, 0, 0};
     unsigned long long neg_mn = 0;
+    const long long w_lo = d.window_start, w_hi = d.window_start + d.active_size;
     const long long stride = (long long)gridDim.x * blockDim.x;
     for (long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x; c < d.domain_size; c += stride) {
         const int t = d.cell_type[c];
         const int ly = d.layer_id[c];
         const int cts = d.crit_time_step[c];
-        if (ly == 0) {
+        if (ly == d.layer) {
             if (t == kLiquid) {
                 if (cts > d.cycle)
                     a[0]++;
                 else
                     a[1]++;
                 const unsigned long long neg = ~(unsigned long long)(long long)cts;
-                if (c < d.active_size && neg > neg_mn)
+                if (c >= w_lo && c < w_hi && neg > neg_mn)
                     neg_mn = neg;
             }
             else if (t == kActive)
@@ -144,17 +147,25 @@ void census_cells(int device, void *stream, const exaca_cell_fields *domains, in
         largest = domains[i].domain_size > largest ? domains[i].domain_size : largest;
     unsigned char *desc = s.ptr;
     unsigned long long *acc = reinterpret_cast<unsigned long long *>(s.ptr + kAccOffset);
-    check(cudaMemcpyAsync(desc, domains, n_domains * kDescBytes, cudaMemcpyHostToDevice, st), "descriptor copy");
-    check(cudaMemsetAsync(acc, 0, n_domains * kAccWords * sizeof(unsigned long long), st), "accumulator clear");
-    long long bx = (4ll * s.num_sms + n_domains - 1) / n_domains;
-    const long long need = (largest + kThreads - 1) / kThreads;
-    bx = bx < need ? bx : need;
-    bx = bx < 1 ? 1 : bx;
-    k_census_cells<<<dim3((unsigned)bx, (unsigned)n_domains), kThreads, 0, st>>>(
-        reinterpret_cast<const exaca_cell_fields *>(desc), acc);
-    check(cudaGetLastError(), "k_census_cells launch");
-    check(cudaMemcpyAsync(out, acc, n_domains * sizeof(exaca_census), cudaMemcpyDeviceToHost, st), "census copy");
-    check(cudaStreamSynchronize(st), "census stream");
+    try {
+        check(cudaMemcpyAsync(desc, domains, n_domains * kDescBytes, cudaMemcpyHostToDevice, st), "descriptor copy");
+        check(cudaMemsetAsync(acc, 0, n_domains * kAccWords * sizeof(unsigned long long), st), "accumulator clear");
+        long long bx = (4ll * s.num_sms + n_domains - 1) / n_domains;
+        const long long need = (largest + kThreads - 1) / kThreads;
+        bx = bx < need ? bx : need;
+        bx = bx < 1 ? 1 : bx;
+        k_census_cells<<<dim3((unsigned)bx, (unsigned)n_domains), kThreads, 0, st>>>(
+            reinterpret_cast<const exaca_cell_fields *>(desc), acc);
+        check(cudaGetLastError(), "k_census_cells launch");
+        check(cudaMemcpyAsync(out, acc, n_domains * sizeof(exaca_census), cudaMemcpyDeviceToHost, st), "census copy");
+        check(cudaStreamSynchronize(st), "census stream");
+    }
+    catch (...) {
+        // work of this call may still be queued on the stream: the lock (which keeps other calls off
+        // the shared array) is released only once it has drained
+        cudaStreamSynchronize(st);
+        throw;
+    }
     for (int i = 0; i < n_domains; i++)
         out[i].next_cts = ~out[i].next_cts;
 }

@@ -36,7 +36,8 @@ def serve(requests: list, device: int = 0, budget_bytes: int = 150 * 10**9, chun
           list_capacity: int = 1 << 27, init_threads: int | None = None, keep_results: bool = False,
           deadline_s: float | None = None, pool_factory=Pool) -> dict:
     """Runs the request loop in real time and returns per-request latencies (s, arrival to result
-    on the host), completion order and, with keep_results, each GrainID / CellType / final cycle.
+    on the host), completion order and, with keep_results, each GrainID / CellType / final cycle
+    (keep_results True: every request's; a set of request indices: those requests' only).
 
     deadline_s: a request whose result is not on the host that many seconds after its arrival is
     given up (its slot retired while the others run on, or never admitted); it is listed in
@@ -119,7 +120,7 @@ def serve(requests: list, device: int = 0, budget_bytes: int = 150 * 10**9, chun
                 g, c = pool.copy_out_concurrent(slot)
                 pool.retire(slot)
                 latency[k] = time.perf_counter() - t_start - requests[k][0]
-                if keep_results:
+                if keep_results is True or (keep_results and k in keep_results):
                     results[k] = (g, c, cycle)
                 done_count += 1
             finished = []

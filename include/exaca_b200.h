@@ -169,6 +169,13 @@ int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c);
  * 1000-cycle census, termination, type-S cycle jump; progress lines are appended to stdout when
  * verbose is 1. */
 int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cycle);
+/* Ends the current layer of a multilayer slot and sets up the next: DomainShiftAndResize (the new
+ * window from one plane below the lowest active cell to the highest cell of the next layer) and
+ * LayerSetup (window octahedra cleared, fresh octahedra for its active cells), as the reference's
+ * layer loop does between layers (src/runCA.cpp:344-390; src/CAinitialize.cpp:2772-2982); the
+ * cycle restarts at 0. The reference's lines are appended to stdout when verbose is 1.
+ * EXACA_ERR_ARG if the slot is in its last layer. */
+int exaca_pool_next_layer(exaca_pool *pool, int slot, int verbose);
 /* CUDA-event device time (ms) of the last exaca_pool_run_plain on this pool. */
 double exaca_pool_last_run_ms(exaca_pool *pool);
 /* Runs n_cycles cycles pass by pass as separate kernels with CUDA events around each launch and
@@ -226,7 +233,7 @@ int exaca_problem_write_outputs(const exaca_problem *p, const int32_t *grain_id,
  * the caller holds in device memory, for callers that must not allocate device memory: a monitor
  * sampling solves that are still running (cudaMalloc / cudaFree may synchronise the device and
  * stall them) or a server whose HBM budget is fully handed out. It allocates nothing: its working
- * data lives in a fixed 24 KiB array in the library's device image (per device), which holds the
+ * data lives in a fixed 26 KiB array in the library's device image (per device), which holds the
  * descriptors and accumulators of at most EXACA_CENSUS_MAX_DOMAINS domains per call; larger
  * n_domains returns EXACA_ERR_ARG. Each field pointer is a CUDA device pointer on `device`, indexed
  * like the pool's fields (k*mx*my + i*my + j); cell_type holds the reference's codes. */
@@ -236,9 +243,14 @@ typedef struct {
     const int8_t *layer_id;        /* domain_size cells */
     const int32_t *crit_time_step; /* domain_size cells */
     int64_t domain_size;           /* cells */
-    int64_t active_size;           /* cells of the active window (next_cts is taken over these) */
+    int64_t active_size;           /* cells of the active window (nzActive planes) */
     int32_t cycle;                 /* the CA cycle the census is taken at */
-    int32_t reserved;              /* 0 */
+    int32_t layer;                 /* the current layer (layernumber): its cells are counted as
+                                      superheated / undercooled / active / solid, liquid cells of
+                                      other layers as remaining (src/CAupdate.cpp:741-757) */
+    int64_t window_start;          /* first cell of the active window, ZBound_Low * mx * my: next_cts
+                                      is taken over [window_start, window_start + active_size)
+                                      (src/CAupdate.cpp:792-805) */
 } exaca_cell_fields;
 /* Writes out[i] for domains[i], i < n_domains, equal to what exaca_pool_census reports for a slot
  * holding the same fields at the same cycle. `stream` is a cudaStream_t (NULL: the legacy default

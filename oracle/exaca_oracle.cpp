@@ -19,12 +19,16 @@
 //   int  oracle_geometry(void *o, long long *out6)    mx, my, nz, nz_active, domain size, active size
 //                                                      (of the current layer's window)
 //   int  oracle_step(void *o, int n_cycles)            n raw cycles of the current layer (no check)
+//   int  oracle_run_to(void *o, int stop, int *final)   the same, paused (returns 1) after cycle `stop`
 //   int  oracle_run(void *o, int *final_cycle)          to termination of the last layer, as
 //                                                      RunProgram_Reduced does
 //   int  oracle_cycle(void *o)
+//   void oracle_set_threads(int n)                     host threads of CellCapture's first pass
+//   int  oracle_census(void *o, long long *out, int max)  censuses of oracle_run (6 numbers each)
 //   int  oracle_fields(void *o, int *cell_type, int *grain_id, float *dl, float *doc, float *cdl)
 //   void oracle_free(void *o)
 #include <algorithm>
+#include <array>
 #include <climits>
 #include <cmath>
 #include <cstdio>
@@ -43,6 +47,8 @@ enum { Wall = 0, Solid = 1, Active = 2, TemporaryUpdate = 3, TemporaryInit = 4, 
 const int NGrainOrientations = 10000;
 
 thread_local std::string g_error;
+// host threads of the dense first pass of CellCapture (oracle_set_threads; 1 = plain serial loop)
+int g_threads = 1;
 
 // ---- input file (src/CAinitialize.cpp:24-576) ---------------------------------------------------
 struct Input {
@@ -384,8 +390,12 @@ struct Oracle {
     std::vector<int> NucleiLocation, NucleationTimes;
     double A, B, C, D;
     int cycle = 0, nn = 0, layer = 0;
+    bool layer_started = false; // the layer loop of oracle_run_to is inside layer `layer`
     std::vector<int> finish; // type R: per layer, FinishTimeStep
     std::vector<int> SteeringVector;
+    // every census of the layer loop (oracle_run): cycle, superheated, undercooled, nucleation events,
+    // remaining liquid, and the cycle jumped to (0: no jump)
+    std::vector<std::array<long long, 6>> census;
 
     long idx(int k, int i, int j) const { return (long)k * MX * MY + (long)i * MY + j; }
 };
@@ -838,18 +848,50 @@ void capture(Oracle &o, long D3D1, long Nb, long GlobalNb, int RankX, int RankY,
 }
 
 // src/CAupdate.cpp:204-728 with the Serial backend's ascending order
+// First pass of CellCapture (src/CAupdate.cpp:217-242) over window cells [lo, hi): undercooling
+// update, and the active cells listed in ascending order. Cells are independent in this pass, so
+// contiguous ranges may run on separate threads; their lists, joined in range order, are the Serial
+// backend's steering vector.
+int pass1_range(Oracle &o, long lo, long hi, int *steer) {
+    // the window index D3D1 maps to the global index D3D1 + ZBound_Low * MX * MY
+    const long shift = (long)o.ZBound_Low * o.MX * o.MY;
+    const int *ctype = o.CellType.data() + shift, *layer = o.LayerID.data() + shift,
+              *cts = o.CritTimeStep.data() + shift;
+    float *u = o.UndercoolingCurrent.data() + shift;
+    const float *du = o.UndercoolingChange.data() + shift;
+    const int lay = o.layer, cycle = o.cycle;
+    int n = 0;
+    for (long D3D1 = lo; D3D1 < hi; D3D1++) {
+        int ct = ctype[D3D1];
+        if (layer[D3D1] <= lay && ct != Solid && cycle > cts[D3D1]) {
+            u[D3D1] += du[D3D1] * ((ct == Liquid) + (ct == Active));
+            if (ct == Active)
+                steer[n++] = (int)D3D1;
+        }
+    }
+    return n;
+}
+
 void cell_capture(Oracle &o) {
     const int MX = o.MX, MY = o.MY;
     int numSteer = 0;
-    for (long D3D1 = 0; D3D1 < o.NA; D3D1++) {
-        int RankZ = D3D1 / (MX * MY);
-        int Rem = D3D1 % (MX * MY);
-        long Global = (long)(RankZ + o.ZBound_Low) * MX * MY + Rem;
-        int ct = o.CellType[Global];
-        if (o.LayerID[Global] <= o.layer && ct != Solid && o.cycle > o.CritTimeStep[Global]) {
-            o.UndercoolingCurrent[Global] += o.UndercoolingChange[Global] * ((ct == Liquid) + (ct == Active));
-            if (ct == Active)
-                o.SteeringVector[numSteer++] = (int)D3D1;
+    if (g_threads <= 1) {
+        numSteer = pass1_range(o, 0, o.NA, o.SteeringVector.data());
+    }
+    else {
+        // range t lists into SteeringVector from its own start lo_t (a range lists at most its own
+        // cells), then the lists are moved down to be contiguous, in range order
+        const int T = g_threads;
+        std::vector<int> count(T);
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+        for (int t = 0; t < T; t++) {
+            const long lo = o.NA * t / T, hi = o.NA * (t + 1) / T;
+            count[t] = pass1_range(o, lo, hi, o.SteeringVector.data() + lo);
+        }
+        for (int t = 0; t < T; t++) {
+            const long lo = o.NA * t / T;
+            std::memmove(o.SteeringVector.data() + numSteer, o.SteeringVector.data() + lo, sizeof(int) * count[t]);
+            numSteer += count[t];
         }
     }
     for (int num = 0; num < numSteer; num++) {
@@ -896,6 +938,11 @@ int check(Oracle &o) {
             else
                 uc++;
         }
+    unsigned long rem = 0;
+    for (long p = 0; p < o.N; p++)
+        if (o.LayerID[p] != o.layer && o.CellType[p] == Liquid)
+            rem++;
+    o.census.push_back({(long long)o.cycle, (long long)sh, (long long)uc, (long long)o.nn, (long long)rem, 0});
     if (sh + uc == 0)
         return 1;
     if ((o.in.type == "S" || o.in.type == "R") && uc == 0) {
@@ -906,8 +953,10 @@ int check(Oracle &o) {
             if (o.CellType[g] == Liquid && o.LayerID[g] == o.layer && cts < next)
                 next = cts;
         }
-        if ((next - o.cycle) > 5000)
+        if ((next - o.cycle) > 5000) {
             o.cycle = next - 1;
+            o.census.back()[5] = (long long)next;
+        }
         // src/CAupdate.cpp:818-819
         if (o.in.type == "R" && o.cycle >= o.finish[o.layer])
             return 1;
@@ -994,19 +1043,28 @@ int oracle_step(void *p, int n) {
     return 0;
 }
 
-// src/runCA.cpp:282-411: every layer's cycles, the window moved between layers
-int oracle_run(void *p, int *final_cycle) {
+// src/runCA.cpp:282-411: every layer's cycles, the window moved between layers. Stops early (returns
+// 1) once a cycle equal to stop_cycle has run; a later call resumes the same layer loop.
+int oracle_run_to(void *p, int stop_cycle, int *final_cycle) {
     Oracle &o = *static_cast<Oracle *>(p);
     for (; o.layer < o.in.layers; o.layer++) {
+        if (!o.layer_started) {
+            o.nn = 0;
+            o.layer_started = true;
+        }
         int XSwitch = 0;
-        o.nn = 0;
         do {
             o.cycle++;
             nucleation(o);
             cell_capture(o);
             if (o.cycle % 1000 == 0)
                 XSwitch = check(o);
+            if (XSwitch == 0 && o.cycle == stop_cycle) {
+                *final_cycle = o.cycle;
+                return 1;
+            }
         } while (XSwitch == 0);
+        o.layer_started = false;
         if (o.layer != o.in.layers - 1) {
             domain_shift_and_resize(o);
             layer_setup(o);
@@ -1018,7 +1076,22 @@ int oracle_run(void *p, int *final_cycle) {
     return 0;
 }
 
+int oracle_run(void *p, int *final_cycle) { return oracle_run_to(p, INT_MIN, final_cycle); }
+
 int oracle_cycle(void *p) { return static_cast<Oracle *>(p)->cycle; }
+
+// host threads of CellCapture's dense first pass (results do not depend on it)
+void oracle_set_threads(int n) { g_threads = n < 1 ? 1 : n; }
+
+// the censuses of oracle_run so far, 6 numbers each (cycle, superheated, undercooled, nucleation
+// events, remaining liquid, cycle jumped to or 0); copies up to max of them, returns how many exist
+int oracle_census(void *p, long long *out, int max) {
+    Oracle &o = *static_cast<Oracle *>(p);
+    for (int q = 0; q < max && q < (int)o.census.size(); q++)
+        for (int f = 0; f < 6; f++)
+            out[6 * q + f] = o.census[q][f];
+    return (int)o.census.size();
+}
 
 int oracle_fields(void *p, int *cell_type, int *grain_id, float *dl, float *doc, float *cdl) {
     Oracle &o = *static_cast<Oracle *>(p);

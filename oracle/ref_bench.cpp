@@ -5,7 +5,11 @@
 // consecutive samples of `cycles_per_sample` cycles each with a steady clock. It prints one JSON
 // object with the time of every sample.
 //
-//   ref_bench <input file> <samples> <cycles_per_sample>
+//   ref_bench <input file> <samples> <cycles_per_sample> [dump file]
+//
+// With a dump file, the final GrainID and CellType (int32, LocalDomainSize each, in that order)
+// are written there raw. Built with Serial dispatch (ref_bench_serial) this pins the restatement
+// at a given cycle on domains too large for a complete reference run.
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -19,7 +23,7 @@
 
 int main(int argc, char **argv) {
     if (argc < 4) {
-        std::fprintf(stderr, "usage: ref_bench <input file> <samples> <cycles_per_sample>\n");
+        std::fprintf(stderr, "usage: ref_bench <input file> <samples> <cycles_per_sample> [dump file]\n");
         return 2;
     }
     std::string input = argv[1];
@@ -142,6 +146,15 @@ int main(int argc, char **argv) {
                                                LayerID);
             }
             sample_s.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count());
+        }
+        if (argc > 4) {
+            FILE *f = std::fopen(argv[4], "wb");
+            if (!f || std::fwrite(GrainID.data(), sizeof(int), LocalDomainSize, f) != (size_t)LocalDomainSize ||
+                std::fwrite(CellType.data(), sizeof(int), LocalDomainSize, f) != (size_t)LocalDomainSize) {
+                std::fprintf(stderr, "cannot write %s\n", argv[4]);
+                return 1;
+            }
+            std::fclose(f);
         }
         int threads = 1;
 #ifdef EXACA_SHIM_OPENMP

@@ -14,8 +14,11 @@ tests/golden/inputs/, and stores per case in tests/golden/<case>.npz:
                DOCenter / CritDiagonalLength over cells with DL != 0
   cycle        the final cycle written to the .log
   census       the reference's every-1000-cycle stdout lines
+  log          the reference's .log file (its timing values vary from run to run)
+  stdout       the reference's whole stdout
 
-Needs /root/reference (build container only). Usage: python tests/golden/make_golden.py [case ...]
+Needs the reference sources (build container only; oracle/Makefile REF). Usage:
+    python tests/golden/make_golden.py [case ...]
 """
 import hashlib
 import os
@@ -86,7 +89,9 @@ def run_case(case):
         env = dict(os.environ, EXACA_SHIM_DUMP_DIR=dump)
         r = subprocess.run([REF, inp], cwd=work, env=env, capture_output=True, text=True, check=True)
         dbg = parse_vtk(os.path.join(work, base + "_debug.vtk"))
-        census = [ln for ln in r.stdout.splitlines() if ln.startswith("cycle =") or ln.startswith("Jumping")]
+        # census and jump lines, in order (a census line may follow text printed without a line break)
+        census = [m.group(0) for m in re.finditer(r"cycle = \d+ Superheated.*|^Jumping to cycle \d+", r.stdout,
+                                                  re.MULTILINE)]
         log = open(os.path.join(work, base + ".log")).read()
         cycle = int(re.search(r"output written at cycle (\d+)", log).group(1))
         gid = np.fromfile(os.path.join(dump, "GrainID.bin"), np.int32)
@@ -118,6 +123,8 @@ def run_case(case):
             sha_cdl=sha(np.ascontiguousarray(cdl[ever]).tobytes()),
             cycle=np.int64(cycle),
             census=np.array(census),
+            log=np.array(log),
+            stdout=np.array(r.stdout),
         )
         np.savez_compressed(os.path.join(HERE, case + ".npz"), **out)
         print(f"{case}: cycle {cycle}, {gid.size} cells, {len(census)} census lines")

@@ -24,6 +24,9 @@ def lib():
         L.oracle_geometry.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]
         L.oracle_step.argtypes = [ctypes.c_void_p, ctypes.c_int]
         L.oracle_run.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_run_to.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_int)]
+        L.oracle_set_threads.argtypes = [ctypes.c_int]
+        L.oracle_census.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong), ctypes.c_int]
         L.oracle_cycle.argtypes = [ctypes.c_void_p]
         L.oracle_fields.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 5
         _lib = L
@@ -46,6 +49,31 @@ class Oracle:
         c = ctypes.c_int()
         lib().oracle_run(self.h, ctypes.byref(c))
         return c.value
+
+    def run_to(self, stop_cycle):
+        """The layer loop of run(), paused after cycle stop_cycle; True if it paused there."""
+        c = ctypes.c_int()
+        return lib().oracle_run_to(self.h, stop_cycle, ctypes.byref(c)) == 1
+
+    @staticmethod
+    def set_threads(n):
+        """Host threads of CellCapture's dense first pass (the results do not depend on it)."""
+        lib().oracle_set_threads(n)
+
+    def census_lines(self):
+        """The stdout lines the reference prints at the censuses run so far (src/CAupdate.cpp:776-780, 815)."""
+        n = lib().oracle_census(self.h, None, 0)
+        buf = (ctypes.c_longlong * (6 * max(n, 1)))()
+        lib().oracle_census(self.h, buf, n)
+        out = []
+        for q in range(n):
+            cyc, sh, uc, nn, rem, jump = buf[6 * q: 6 * q + 6]
+            out.append(f"cycle = {cyc} Superheated liquid cells = {sh} Undercooled liquid cells = {uc} "
+                       f"Number of nucleation events this layer {nn} Remaining liquid cells in future layers of "
+                       f"this simulation = {rem}")
+            if jump:
+                out.append(f"Jumping to cycle {jump}")
+        return out
 
     @property
     def cycle(self):

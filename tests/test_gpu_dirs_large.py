@@ -1,0 +1,80 @@
+"""The benchmark's directional-solidification workload at full size (256^3 and 512^3, G = R = 1e6,
+N = 25, 1e14 m^-3 nuclei), pinned without dense fixtures: SHA-256 digests of GrainID (int32) and
+CellType (int8) over the whole cell array, stored in tests/golden/DirS<n>.json by
+tests/golden/make_dirs512.py.
+
+* after 5000 cycles: the unmodified reference (Serial order) and the oracle's restatement agree on
+  these digests; the CUDA solver must give the same;
+* at termination: the restatement's digests, final cycle and census lines (the reference itself
+  cannot run the 512^3 solve to its end: its 32-bit `26 * D3D1ConvPosition`, src/CAupdate.cpp:336,
+  overflows once active cells lie above z ~ 310).
+
+Scale-specific paths are exercised here that the small golden cases do not reach: 32-bit cell
+indices in the claim words and claim lists, list and shard capacities, growth tables of ~16,000
+entries, and 1.1 GB result copies."""
+import hashlib
+import json
+import os
+import re
+
+import numpy as np
+import pytest
+
+from helpers import GOLDEN
+
+import exaca_b200 as ex
+
+pytestmark = pytest.mark.gpu
+
+CASES = sorted(f[:-5] for f in os.listdir(GOLDEN) if re.fullmatch(r"DirS\d+\.json", f))
+
+
+def digests(grain_id, cell_type):
+    return {"sha_grain_id": hashlib.sha256(np.ascontiguousarray(grain_id, dtype=np.int32).tobytes()).hexdigest(),
+            "sha_cell_type": hashlib.sha256(np.ascontiguousarray(cell_type).astype(np.int8).tobytes()).hexdigest()}
+
+
+@pytest.fixture(scope="module", params=CASES)
+def case(request, tmp_path_factory):
+    pin = json.load(open(os.path.join(GOLDEN, request.param + ".json")))
+    inp = tmp_path_factory.mktemp(request.param) / "input.txt"
+    inp.write_text("\n".join(pin["input"]) + "\n")
+    prob = ex.Problem.from_file(str(inp))
+    return pin, prob
+
+
+def test_pinned_cycle_equals_reference(lib, case):
+    pin, prob = case
+    ref = pin["cycle5000_reference"]
+    assert ref["sha_grain_id"] == pin["cycle5000_restatement"]["sha_grain_id"]
+    assert ref["sha_cell_type"] == pin["cycle5000_restatement"]["sha_cell_type"]
+    pool = ex.Pool(0, list_capacity=prob.geometry.active_size)
+    try:
+        slot = pool.admit(prob, device_check=False)
+        pool.step(pin["pin_cycle"])
+        st = pool.status(slot)
+        assert st.cycle == pin["pin_cycle"] and st.error == 0
+        gid, ct = pool.copy_out(slot)
+        assert gid.size == ref["cells"]
+        assert digests(gid, ct) == {k: ref[k] for k in ("sha_grain_id", "sha_cell_type")}
+    finally:
+        pool.close()
+
+
+def test_full_solve_equals_restatement(lib, case, capfd):
+    pin, prob = case
+    fin = pin["final"]
+    pool = ex.Pool(0, list_capacity=prob.geometry.active_size)
+    try:
+        slot = pool.admit(prob, device_check=False)
+        capfd.readouterr()
+        cycle = pool.run_plain(slot, verbose=True)
+        out = capfd.readouterr().out
+        assert cycle == fin["cycle"]
+        census = [m.group(0) for m in re.finditer(r"cycle = \d+ Superheated.*", out)]
+        assert census == fin["census"]
+        gid, ct = pool.copy_out(slot)
+        assert digests(gid, ct) == {k: fin[k] for k in ("sha_grain_id", "sha_cell_type")}
+        assert pool.status(slot).error == 0
+    finally:
+        pool.close()

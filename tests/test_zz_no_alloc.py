@@ -21,6 +21,10 @@ def test_rejects_more_domains_than_the_scratch_holds(lib):
 
 
 def device_domain(torch, pool, slot, prob, keep):
+    """Caller-owned device copies of a slot's CellType (read back from the device) and of its LayerID
+    and CritTimeStep. The reference assigns LayerID and CritTimeStep to every cell of every layer at
+    initialisation and never changes them (the layer loop, src/runCA.cpp:344-405, moves the window
+    only), so the problem's initial fields are the slot's; CellType changes every cycle."""
     _, ct = pool.copy_out(slot)
     f = prob.fields()
     t = {
@@ -30,8 +34,11 @@ def device_domain(torch, pool, slot, prob, keep):
     }
     keep.append(t)  # the tensors outlive the census call
     g = prob.geometry
+    st = pool.status(slot)
+    plane = g.mx * g.my
     d = {k: v.data_ptr() for k, v in t.items()}
-    d.update(domain_size=g.domain_size, active_size=g.active_size, cycle=pool.status(slot).cycle)
+    d.update(domain_size=g.domain_size, active_size=st.window_nz * plane, cycle=st.cycle, layer=st.layer,
+             window_start=st.window_z_lo * plane)
     return d
 
 
@@ -59,5 +66,48 @@ def test_census_cells_equals_pool_census_twice(lib):
             # the same call again on the state the previous call left in the scratch array
             assert ex.census_cells(0, doms, stream=stream) == want
             assert ex.census_cells(0, doms[1:], stream=0) == want[1:]
+    finally:
+        pool.close()
+
+
+@pytest.mark.gpu
+def test_census_cells_in_a_later_layer(lib):
+    """A three-layer spot melt stepped into its second layer: the layer number selects the cells that
+    are classified (the first layer's are neither counted nor remaining once solid), and the window
+    start bounds the cells the next CritTimeStep is taken over; both must equal the pool's census."""
+    import torch
+
+    prob = ex.Problem.from_file(input_path("SpotMelt3Layers"))
+    pool = ex.Pool(0, list_capacity=prob.geometry.domain_size)
+    slot = pool.admit(prob, device_check=False)
+    stream = torch.cuda.current_stream().cuda_stream
+    try:
+        # layer 0 to its end as the plain driver's census finds it (idle cycles instead of its jump)
+        for _ in range(200):
+            pool.step(1000)
+            c = pool.census(slot)
+            if c["superheated"] + c["undercooled"] == 0:
+                break
+        else:
+            pytest.fail("layer 0 did not end within 200000 cycles")
+        pool.next_layer(slot)
+        st = pool.status(slot)
+        assert st.layer == 1 and st.window_z_lo > 0
+        checked = 0
+        for _ in range(60):
+            pool.step(500)
+            want = pool.census(slot)
+            keep = []
+            dom = device_domain(torch, pool, slot, prob, keep)
+            assert ex.census_cells(0, [dom], stream=stream) == [want]
+            assert ex.census_cells(0, [dom], stream=stream) == [want]
+            if want["undercooled"] > 0 and want["active"] > 0 and want["solid"] > 0:
+                checked += 1
+                # the window and layer matter here: the census of layer 0 over the whole domain differs
+                first = dict(dom, layer=0, window_start=0)
+                assert ex.census_cells(0, [first], stream=stream) != [want]
+            if checked >= 2:
+                break
+        assert checked >= 2, "layer 1 never held undercooled, active and solid cells together"
     finally:
         pool.close()
