@@ -20,9 +20,11 @@ LIB = os.path.join(HERE, "lib")
 OBJ = os.path.join(HERE, "_build")
 ROOT = os.path.dirname(HERE)
 
-HOST_SOURCES = ["input.cpp", "init.cpp", "output.cpp", "capi.cpp"]
+HOST_SOURCES = ["input.cpp", "init.cpp", "output.cpp", "capi.cpp", "rng.cpp"]
+# per-file optimisation level (the random-stream refill is vectorised at -O3)
+HOST_OPT = {"rng.cpp": "-O3"}
 CUDA_SOURCES = ["device.cu", "census_scratch.cu"]
-HEADERS = ["exaca_host.hpp", "pool.hpp"]
+HEADERS = ["exaca_host.hpp", "pool.hpp", "rng.hpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXX = "g++"
@@ -52,7 +54,8 @@ def build(verbose=False):
         src = os.path.join(SRC, s)
         obj = os.path.join(OBJ, s + ".o")
         if _newer(obj, [src] + hdrs):
-            _run([CXX] + HOST_FLAGS + ["-c", src, "-o", obj])
+            flags = [HOST_OPT.get(s, f) if f == "-O2" else f for f in HOST_FLAGS]
+            _run([CXX] + flags + ["-c", src, "-o", obj])
         objs.append(obj)
     for s in CUDA_SOURCES:
         src = os.path.join(SRC, s)

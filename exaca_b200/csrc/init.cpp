@@ -1,12 +1,14 @@
 // Host-side problem set-up for the B200 solver: geometry, temperature field, substrate, grain seeds,
 // nuclei, and the lookup tables the device kernels use.
 //
-// The random streams are the reference's (libstdc++ mt19937_64 / uniform_real_distribution,
-// default_random_engine / normal_distribution) drawn in the reference's loop orders, so the same
-// input file yields the same seeds and nuclei. Everything that is a pure per-cell function of these
+// The random streams are the reference's (libstdc++ mt19937_64 / uniform_real_distribution, drawn
+// through the bit-identical Mt64 / uniform01 of rng.hpp; default_random_engine /
+// normal_distribution) drawn in the reference's loop orders, so the same input file yields the same
+// seeds and nuclei. Everything that is a pure per-cell function of these
 // (the fresh-octahedron state of initially active cells, the Voronoi baseplate) is finished on the
 // device when the problem is admitted to a pool.
 #include "exaca_host.hpp"
+#include "rng.hpp"
 
 #include <algorithm>
 #include <cctype>
@@ -14,8 +16,12 @@
 #include <cmath>
 #include <cstring>
 #include <fstream>
+#include <future>
+#include <map>
+#include <mutex>
 #include <random>
 #include <sstream>
+#include <sys/stat.h>
 
 namespace exaca {
 
@@ -139,6 +145,37 @@ void build_cdl_table(const std::vector<float> &guv, std::vector<float> &table) {
         }
     }
 }
+
+namespace {
+
+// The orientation file's unit vectors and fresh-octahedron critical lengths depend on the file
+// alone, so they are read and tabulated once per process for each file (path, size and modification
+// time) and shared by every problem that names it.
+struct OrientationTables {
+    std::vector<float> guv, cdl_table;
+};
+
+std::shared_ptr<const OrientationTables> orientation_tables(const std::string &path) {
+    static std::mutex mu;
+    static std::map<std::string, std::shared_ptr<const OrientationTables>> cache;
+    struct stat st;
+    std::string key = path;
+    if (stat(path.c_str(), &st) == 0)
+        key += "|" + std::to_string((long long)st.st_size) + "|" + std::to_string((long long)st.st_mtime);
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it != cache.end())
+            return it->second;
+    }
+    auto t = std::make_shared<OrientationTables>();
+    read_orientations(path, t->guv);
+    build_cdl_table(t->guv, t->cdl_table);
+    std::lock_guard<std::mutex> lock(mu);
+    return cache.emplace(key, t).first->second;
+}
+
+} // namespace
 
 void build_growth_table(const Problem &p, int n_entries, std::vector<double> &growth) {
     growth.resize(n_entries);
@@ -578,8 +615,7 @@ void temp_init_reduced(Problem &p, const TemperatureData &td, std::string &log) 
 // src/CAinitialize.cpp:1460-1529 (np = 1: rank seed 0, grain IDs 1, 2, ... in index order)
 void substrate_constrained(Problem &p) {
     Geometry &g = p.g;
-    std::mt19937_64 gen(0);
-    std::uniform_real_distribution<double> dis(0.0, 1.0);
+    Mt64 gen(0);
     for (int k = 0; k < g.nz; k++) {
         for (int i = 0; i < g.mx; i++) {
             for (int j = 0; j < g.my; j++) {
@@ -590,7 +626,7 @@ void substrate_constrained(Problem &p) {
                     p.grain_id[idx] = 0;
                 }
                 else if (k == 1 && i > 0 && i < g.mx - 1 && j > 0 && j < g.my - 1) {
-                    double r = dis(gen);
+                    double r = uniform01(gen.next());
                     p.cell_type[idx] = r < p.cfg.fract_surface_sites_active ? kActive : kLiquid;
                 }
                 else {
@@ -614,15 +650,14 @@ namespace {
 void substrate_from_spacing(Problem &p, std::vector<int32_t> &seeds, std::string &log) {
     Geometry &g = p.g;
     const InputConfig &c = p.cfg;
-    std::mt19937_64 gen(1.0);
-    std::uniform_real_distribution<double> dis(0.0, 1.0);
+    Mt64 gen((uint64_t)1.0); // std::mt19937_64 gen(1.0)
     float sp = c.substrate_grain_spacing;
     double prob = (c.deltax * c.deltax * c.deltax) / (sp * sp * sp * pow(10, -18));
     seeds.clear();
     for (int k = 1; k <= g.nz_active; k++)
         for (int i = 1; i < g.nx - 1; i++)
             for (int j = 1; j < g.ny - 1; j++) {
-                double r = dis(gen);
+                double r = uniform01(gen.next());
                 if (r < prob) {
                     seeds.push_back(i);
                     seeds.push_back(j);
@@ -704,8 +739,7 @@ void active_cell_wall_init(Problem &p, const int it[9][26], const int lens[9], s
 // per-cell function of (position, GrainID) and is filled in on the device at admission.
 void grain_init(Problem &p, const int it[9][26], const int lens[9], std::string &log) {
     Geometry &g = p.g;
-    std::mt19937_64 gen(0);
-    std::uniform_real_distribution<double> dis(0.0, 1.0);
+    Mt64 gen(0);
     double bulk_prob = p.cfg.nmax * p.cfg.deltax * p.cfg.deltax * p.cfg.deltax;
     int possible = 0;
     for (int k = 1; k < g.nz - 1; k++)
@@ -713,7 +747,7 @@ void grain_init(Problem &p, const int it[9][26], const int lens[9], std::string 
             for (int i = 1; i < g.mx - 1; i++) {
                 long idx = cell_index(g, k, i, j);
                 if (p.cts[idx] != 0) {
-                    double r = dis(gen);
+                    double r = uniform01(gen.next());
                     if (r < bulk_prob) {
                         possible++;
                         p.cell_type[idx] = kTemporaryInit;
@@ -782,28 +816,38 @@ void init_directional_seeds(Problem &p, std::string & /* log: type C adds no not
     p.du_value = c.R * c.deltat;
     // substrate: one draw per cell of plane k = 1 inside the ghost ring, in (i, j) order
     {
-        std::mt19937_64 gen(0);
-        std::uniform_real_distribution<double> dis(0.0, 1.0);
+        Mt64 gen(0);
         d.active.clear();
         for (int i = 1; i < g.mx - 1; i++)
             for (int j = 1; j < g.my - 1; j++)
-                if (dis(gen) < c.fract_surface_sites_active)
+                if (uniform01(gen.next()) < c.fract_surface_sites_active)
                     d.active.push_back(cell_index(g, 1, i, j));
     }
     // potential nuclei: one draw per cell with CritTimeStep != 0, planes k = 1 .. nz-2 in (k, j, i)
     // order; numbered -1, -2, ... in index order
     std::vector<int32_t> sites;
     {
-        std::mt19937_64 gen(0);
-        std::uniform_real_distribution<double> dis(0.0, 1.0);
+        Mt64 gen(0);
         const double bulk_prob = c.nmax * c.deltax * c.deltax * c.deltax;
+        const int ni = g.mx - 2, nj = g.my - 2;
+        const bool by_limit = bulk_prob > 0.0 && bulk_prob <= 0.5;
+        const uint64_t x_lim = by_limit ? uniform01_limit(bulk_prob) : 0;
         for (int k = 1; k < g.nz - 1; k++) {
             if (d.plane_cts[k] == 0)
                 continue;
-            for (int j = 1; j < g.my - 1; j++)
-                for (int i = 1; i < g.mx - 1; i++)
-                    if (dis(gen) < bulk_prob)
-                        sites.push_back((int32_t)cell_index(g, k, i, j));
+            if (by_limit) {
+                // the plane's draws in (j, i) order, scanned for outputs below the probability's limit
+                gen.scan_below((uint64_t)ni * nj, x_lim, [&](uint64_t t) {
+                    const int j = 1 + (int)(t / ni), i = 1 + (int)(t % ni);
+                    sites.push_back((int32_t)cell_index(g, k, i, j));
+                });
+            }
+            else {
+                for (int j = 1; j < g.my - 1; j++)
+                    for (int i = 1; i < g.mx - 1; i++)
+                        if (uniform01(gen.next()) < bulk_prob)
+                            sites.push_back((int32_t)cell_index(g, k, i, j));
+            }
         }
     }
     std::sort(sites.begin(), sites.end());
@@ -887,12 +931,17 @@ void initialize_problem(Problem &p, std::string &log) {
     // per-cell host fields: they are made on the device
     const bool seeds_only = c.simulation_type == "C" && (g.nx > 3 || g.ny > 3 || g.nz > 3);
     if (seeds_only) {
+        // the orientation tables are read (or taken from the process's cache) while the seeds are drawn
+        auto tables = std::async(std::launch::async, orientation_tables, c.orientation_file);
         init_directional_seeds(p, log);
         g.active_size = (long)g.mx * g.my * g.nz_active;
         log += "Done with temperature field initialization, active domain size is " + std::to_string(g.nz_active) +
                " out of " + std::to_string(g.nz) + " cells in the Z direction\n";
-        read_orientations(c.orientation_file, p.guv);
-        build_cdl_table(p.guv, p.cdl_table);
+        {
+            auto t = tables.get();
+            p.guv = t->guv;
+            p.cdl_table = t->cdl_table;
+        }
         log += "Done with orientation initialization \n";
         log += "Number of potential nucleated grains: " + std::to_string(p.nuclei_loc.size()) + "\n";
         log += "Grain struct initialized\n";
@@ -926,8 +975,11 @@ void initialize_problem(Problem &p, std::string &log) {
     log += "Done with temperature field initialization, active domain size is " + std::to_string(g.nz_active) +
            " out of " + std::to_string(g.nz) + " cells in the Z direction\n";
 
-    read_orientations(c.orientation_file, p.guv);
-    build_cdl_table(p.guv, p.cdl_table);
+    {
+        auto t = orientation_tables(c.orientation_file);
+        p.guv = t->guv;
+        p.cdl_table = t->cdl_table;
+    }
     log += "Done with orientation initialization \n";
 
     std::vector<int32_t> seeds;
