@@ -30,6 +30,8 @@ class FakePool:
         self.slots = {}  # slot -> [bytes, cycles needed, cycles run]
         self.retired = []
         self.max_resident = 0
+        self.max_used = 0
+        self.refused = 0
         self.steps = 0
         self.error_after = error_after
         self.closed = False
@@ -38,12 +40,14 @@ class FakePool:
     def admit(self, prob, device_check=True):
         need = prob.slot_bytes()
         if self.used + need > self.budget:
+            self.refused += 1
             raise ex.ExacaError(-4, "admission refused: HBM budget exceeded")
         slot = self.next_slot
         self.next_slot += 1
         self.slots[slot] = [need, 250 * ((prob.geometry.nz + 7) // 8), 0]
         self.used += need
         self.max_resident = max(self.max_resident, len(self.slots))
+        self.max_used = max(self.max_used, self.used)
         return slot
 
     def bytes_in_use(self):
@@ -93,10 +97,12 @@ def test_every_request_completes_and_frees_its_slot(lib):
 def test_admission_waits_for_the_budget(lib):
     reqs = stream(6)
     probs = serve.build_problems([p for _, p in reqs], threads=2)
-    budget = max(p.slot_bytes() for p in probs)  # room for one request at a time
+    budget = max(p.slot_bytes() for p in probs)  # room for the largest request alone
     out, pool = run(reqs, budget_bytes=budget)
     assert out["timed_out"] == [] and all(x is not None for x in out["latency"])
-    assert pool.max_resident == 1 and pool.used == 0
+    # never above the budget; smaller requests may share it, so the loop admits fewer than all six at
+    # once and waits for retirements
+    assert pool.max_used <= budget and pool.max_resident < len(reqs) and pool.used == 0
 
 
 def test_device_error_stops_the_loop(lib):
