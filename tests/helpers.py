@@ -1,4 +1,5 @@
 """Shared helpers of the parity tests (test infrastructure)."""
+import hashlib
 import os
 import subprocess
 import tempfile
@@ -28,8 +29,29 @@ def reference_error(path):
     return ""
 
 
-def golden_cases():
-    return sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+def golden_cases(dense_only=False):
+    """Golden fixture names; dense_only: the cases that store their dense fields (small domains),
+    for tests that need the arrays themselves or run the serial restatement on them."""
+    cases = sorted(f[:-4] for f in os.listdir(GOLDEN) if f.endswith(".npz"))
+    return [c for c in cases if is_dense(load_golden(c))] if dense_only else cases
+
+
+# dtype of each dense golden field, in which its digest is taken for the large cases (make_golden.py)
+DENSE_DTYPES = dict(init_cell_type=np.int8, init_grain_id=np.int32, init_cts=np.int32, init_layer_id=np.int8,
+                    init_melted=np.int8, final_grain_id=np.int32, final_cell_type=np.int8)
+
+
+def is_dense(g):
+    return "final_grain_id" in g.files
+
+
+def field_equal(g, name, arr):
+    """arr equals the golden field `name`: the stored array, or for large cases its shape and the
+    SHA-256 digest of its bytes in the field's dtype."""
+    if name in g.files:
+        return np.array_equal(arr, g[name])
+    a = np.ascontiguousarray(arr, dtype=DENSE_DTYPES[name])
+    return tuple(a.shape) == tuple(g["shape_" + name]) and hashlib.sha256(a.tobytes()).hexdigest() == str(g["sha_" + name])
 
 
 def load_golden(case):

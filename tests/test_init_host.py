@@ -2,7 +2,9 @@
 import numpy as np
 import pytest
 
-from helpers import golden_cases, input_path, load_golden, to_whole
+import hashlib
+
+from helpers import field_equal, golden_cases, input_path, is_dense, load_golden, to_whole
 
 import exaca_b200 as ex
 
@@ -13,11 +15,21 @@ def test_init_fields_match_reference(lib, case):
     p = ex.Problem.from_file(input_path(case))
     f = p.fields()
     shape = p.shape
-    assert np.array_equal(to_whole(f["cell_type"], shape), g["init_cell_type"])
-    assert np.array_equal(to_whole(f["crit_time_step"], shape), g["init_cts"])
-    assert np.array_equal(to_whole(f["layer_id"], shape), g["init_layer_id"])
+    assert field_equal(g, "init_cell_type", to_whole(f["cell_type"], shape))
+    assert field_equal(g, "init_cts", to_whole(f["crit_time_step"], shape))
+    assert field_equal(g, "init_layer_id", to_whole(f["layer_id"], shape))
     # the debug dump prints UndercoolingChange with %f
-    assert np.allclose(to_whole(f["undercooling_change"], shape), g["init_du"], atol=5e-7, rtol=0)
+    du = to_whole(f["undercooling_change"], shape)
+    if is_dense(g):
+        assert np.allclose(du, g["init_du"], atol=5e-7, rtol=0)
+    else:
+        assert hashlib.sha256(np.ascontiguousarray(du != 0).tobytes()).hexdigest() == str(g["sha_init_du_nonzero"])
+        assert np.allclose(np.unique(du[du != 0]), g["init_du_values"], atol=5e-7, rtol=0)
     gid = to_whole(f["grain_id"], shape)
     pending = gid == ex.VORONOI_PENDING
-    assert np.array_equal(gid[~pending], g["init_grain_id"][~pending])
+    if is_dense(g):
+        assert np.array_equal(gid[~pending], g["init_grain_id"][~pending])
+    elif not pending.any():
+        assert field_equal(g, "init_grain_id", gid)
+    # (a large case with Voronoi-pending substrate cells has its GrainIDs checked after admission on
+    # the device, tests/test_gpu_parity.py)

@@ -17,7 +17,7 @@ def sha_file(path):
         return hashlib.sha256(f.read()).hexdigest()
 
 
-@pytest.mark.parametrize("case", golden_cases())
+@pytest.mark.parametrize("case", golden_cases(dense_only=True))
 @pytest.mark.parametrize("threads", [1, 3, 0])
 def test_output_files_match_reference(case, threads, tmp_path):
     g = load_golden(case)
