@@ -1041,52 +1041,11 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
     }
 }
 
-// Staging of the persistent kernel's growth pass: each warp copies the next iteration's record
-// groups into shared memory with cp.async while it processes the current ones, so the records'
-// global-memory latency is off the pass's chain of dependent rounds without registers to hold them.
-// One group: the four list arrays of 32 consecutive records (1 KB).
-struct GroupStage {
-    ActiveRec rec[32];
-    unsigned int dom[32];
-    unsigned int stat[32];
-    unsigned long long min2[32];
-};
-static_assert(sizeof(GroupStage) == 1024, "a staged group is 64 chunks of 16 bytes");
-// dynamic shared memory of the staged growth pass: per warp two stages of kBatch groups
-template <int kBatch> constexpr int staged_smem_bytes() { return (kBlock / 32) * 2 * kBatch * (int)sizeof(GroupStage); }
-
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-    const unsigned int s = (unsigned int)__cvta_generic_to_shared(smem);
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-// waits until at most one committed group of this thread is still in flight
-__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
-
-// Copies group g of the list into `st` (all lanes of the warp call): 64 chunks of 16 bytes, two per
-// lane. A group at or past the list end is not copied (its records are not read). The list arrays
-// are allocated in whole groups of 32 records, so the copy of the last group stays inside them.
-__device__ __forceinline__ void stage_group(const ActiveRec *in, const unsigned int *in_dom, const unsigned int *in_stat,
-                                            const unsigned long long *in_min2, unsigned long long g,
-                                            unsigned long long n, GroupStage *st, unsigned int lane) {
-    const unsigned long long first = g * 32;
-    if (first >= n)
-        return;
-    cp_async16(&st->rec[lane], in + first + lane);
-    if (lane < 8)
-        cp_async16(&st->dom[4 * lane], in_dom + first + 4 * lane);
-    else if (lane < 16)
-        cp_async16(&st->stat[4 * (lane - 8)], in_stat + first + 4 * (lane - 8));
-    else
-        cp_async16(&st->min2[2 * (lane - 16)], in_min2 + first + 2 * (lane - 16));
-}
-
 // Active records are handed out to warps in groups of 32 consecutive records (one coalesced load),
 // group g to warp g % (number of warps of the grid), consecutive warps on different blocks: the
 // records appended by the last capture pass, which all need a fresh mask and claims, spread over
 // every SM. No block-wide synchronisation.
-template <int kBatch, bool kBlockClaims, bool kStaged = false>
-__device__ void grow_pass(PoolState *P, CycleStats &st, GroupStage *stage = nullptr) {
+template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P, CycleStats &st) {
     const int cur = P->cur;
     const unsigned long long n = P->cnt[cur];
     const unsigned int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1117,34 +1076,13 @@ __device__ void grow_pass(PoolState *P, CycleStats &st, GroupStage *stage = null
     const bool extras = P->extras;
     unsigned long long tombs = 0;
     const unsigned long long groups = (n + 31) / 32;
-    const unsigned long long iter_step = kBatch * nw;
-    // staged: this warp's two stages of kBatch groups; iteration i reads stage i & 1 while the copies
-    // of iteration i + 1 land in the other
-    GroupStage *const wstage = kStaged ? stage + (size_t)warp * 2 * kBatch : nullptr;
-    if (kStaged) {
-#pragma unroll
-        for (int q = 0; q < kBatch; q++)
-            stage_group(in, in_dom, in_stat, in_min2, gw + (unsigned long long)q * nw, n, wstage + q, lane);
-        cp_async_commit();
-    }
-    int buf = 0;
     // records are updated in place; dropped ones become tombstones
-    for (unsigned long long g0 = gw; g0 < groups; g0 += iter_step, buf ^= 1) {
+    for (unsigned long long g0 = gw; g0 < groups; g0 += kBatch * nw) {
         ActiveRec r[kBatch];
         unsigned int dom[kBatch], m[kBatch];
         unsigned long long idx[kBatch], mn2[kBatch];
         double inc[kBatch];
         bool ok[kBatch];
-        if (kStaged) {
-            GroupStage *next = wstage + (buf ^ 1) * kBatch;
-#pragma unroll
-            for (int q = 0; q < kBatch; q++)
-                stage_group(in, in_dom, in_stat, in_min2, g0 + iter_step + (unsigned long long)q * nw, n, next + q,
-                            lane);
-            cp_async_commit();
-            cp_async_wait_all_but_one();
-            __syncwarp();
-        }
 #pragma unroll
         for (int q = 0; q < kBatch; q++) {
             idx[q] = (g0 + (unsigned long long)q * nw) * 32 + lane;
@@ -1153,26 +1091,14 @@ __device__ void grow_pass(PoolState *P, CycleStats &st, GroupStage *stage = null
             m[q] = 0;
             mn2[q] = kNoMin2;
             if (idx[q] < n) {
-                if (kStaged) {
-                    const GroupStage &gs = wstage[buf * kBatch + q];
-                    const int4 v = *reinterpret_cast<const int4 *>(&gs.rec[lane]);
-                    r[q] = *reinterpret_cast<const ActiveRec *>(&v);
-                    dom[q] = gs.dom[lane];
-                    m[q] = gs.stat[lane];
-                    mn2[q] = gs.min2[lane];
-                }
-                else {
-                    // streamed once per cycle: through L2 only
-                    const int4 v = __ldcg(reinterpret_cast<const int4 *>(in + idx[q]));
-                    r[q] = *reinterpret_cast<const ActiveRec *>(&v);
-                    dom[q] = __ldcg(in_dom + idx[q]);
-                    m[q] = __ldcg(in_stat + idx[q]);
-                    mn2[q] = __ldcg(in_min2 + idx[q]);
-                }
+                // streamed once per cycle: through L2 only
+                const int4 v = __ldcg(reinterpret_cast<const int4 *>(in + idx[q]));
+                r[q] = *reinterpret_cast<const ActiveRec *>(&v);
+                dom[q] = __ldcg(in_dom + idx[q]);
+                m[q] = __ldcg(in_stat + idx[q]);
+                mn2[q] = __ldcg(in_min2 + idx[q]);
             }
         }
-        if (kStaged)
-            __syncwarp(); // every lane has read this stage before the next iteration refills it
 #pragma unroll
         for (int q = 0; q < kBatch; q++) {
             inc[q] = 0.0;
@@ -1209,8 +1135,6 @@ __device__ void grow_pass(PoolState *P, CycleStats &st, GroupStage *stage = null
         else
             queue_flagged<kBatch>(P, shard, __popc(flagged), flagged, idx, r, dom, m);
     }
-    if (kStaged)
-        asm volatile("cp.async.wait_all;" ::: "memory"); // no copy is left in flight into the stages
     if (kBlockClaims)
         block_claims(P, bq, shard, st, tombs);
     // dropped records stay as tombstones of the in-place list until the next compaction
@@ -1540,14 +1464,8 @@ template <class F> __device__ bool grid_meet(PoolState *P, int tag, F &&serial) 
     return state != 2;
 }
 
-// Co-resident blocks per SM the persistent kernel is compiled for (its register budget).
-#ifndef EXACA_CYCLES_BLOCKS_PER_SM
-#define EXACA_CYCLES_BLOCKS_PER_SM 2
-#endif
-
 // n_cycles complete CA cycles (start, grow/claim, capture) in one cooperative launch.
-template <int kLanes, int kBatch>
-__global__ void __launch_bounds__(kBlock, EXACA_CYCLES_BLOCKS_PER_SM) k_cycles(PoolState *P, int n_cycles) {
+template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 2) k_cycles(PoolState *P, int n_cycles) {
     CycleStats st;
     // with many domains, their per-cycle start (termination, nucleation) runs across the grid
     // (the descriptors and their number change only between launches)
@@ -1565,12 +1483,10 @@ __global__ void __launch_bounds__(kBlock, EXACA_CYCLES_BLOCKS_PER_SM) k_cycles(P
         begin_domains(P, desc, n_domains, gwarp, nwarp);
         ok = grid_meet(P, -1, [] {});
     }
-    extern __shared__ __align__(16) unsigned char s_dyn[];
-    GroupStage *const stage = reinterpret_cast<GroupStage *>(s_dyn);
     for (int c = 0; ok && c < n_cycles; c++) {
         // growth with each block's claims right after its own growth; the global claim pass only
         // when some block's queue overflowed this cycle (the same answer for every block)
-        grow_pass<kBatch, true, true>(P, st, stage);
+        grow_pass<kBatch, true>(P, st);
         ok = grid_meet(P, 3 * c + 1, [] {});
         if (!ok)
             break;
@@ -1610,14 +1526,12 @@ __global__ void __launch_bounds__(kBlock) k_meet_probe(PoolState *P) {
 // Compiled launch shapes: {capture lanes, growth batch} for kLaneChoices x kBatchChoices.
 struct StepKernels {
     const void *cycles;
-    int cycles_smem; // dynamic shared memory of the persistent kernel (its growth-pass stages)
     void (*grow)(PoolState *);
     void (*capture_begin)(PoolState *);
     void (*capture_end)(PoolState *);
 };
 template <int kL, int kB> StepKernels step_kernels() {
-    return {(const void *)k_cycles<kL, kB>, staged_smem_bytes<kB>(), k_grow<kB>, k_capture_pass<true, kL>,
-            k_capture_pass<false, kL>};
+    return {(const void *)k_cycles<kL, kB>, k_grow<kB>, k_capture_pass<true, kL>, k_capture_pass<false, kL>};
 }
 static_assert(kStepVariants == 4, "two lane widths x two batch depths");
 const StepKernels kStepKernel[kStepVariants] = {
@@ -2013,10 +1927,7 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
         throw DeviceError("device does not support cooperative launches");
     int b = 0;
     for (int v = 0; v < kStepVariants; v++) {
-        CUDA_OK(cudaFuncSetAttribute(kStepKernel[v].cycles, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     kStepKernel[v].cycles_smem));
-        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kStepKernel[v].cycles, kBlock,
-                                                              kStepKernel[v].cycles_smem));
+        CUDA_OK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kStepKernel[v].cycles, kBlock, 0));
         if (b < 1)
             throw DeviceError("persistent kernel does not fit on an SM");
         grid_cycles_[v] = num_sms_ * b;
@@ -2051,13 +1962,11 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
     }
     PoolState ps;
     std::memset(&ps, 0, sizeof(ps));
-    // the list arrays hold whole groups of 32 records (the staged growth pass copies whole groups)
-    const unsigned long long alloc_records = (capacity_ + 31) / 32 * 32;
     for (int q = 0; q < 2; q++) {
-        CUDA_OK(cudaMalloc(&ps.rec[q], alloc_records * sizeof(ActiveRec)));
-        CUDA_OK(cudaMalloc(&ps.rdom[q], alloc_records * sizeof(unsigned int)));
-        CUDA_OK(cudaMalloc(&ps.rstat[q], alloc_records * sizeof(unsigned int)));
-        CUDA_OK(cudaMalloc(&ps.rmin2[q], alloc_records * sizeof(unsigned long long)));
+        CUDA_OK(cudaMalloc(&ps.rec[q], capacity_ * sizeof(ActiveRec)));
+        CUDA_OK(cudaMalloc(&ps.rdom[q], capacity_ * sizeof(unsigned int)));
+        CUDA_OK(cudaMalloc(&ps.rstat[q], capacity_ * sizeof(unsigned int)));
+        CUDA_OK(cudaMalloc(&ps.rmin2[q], capacity_ * sizeof(unsigned long long)));
     }
     // a shard takes the entries of 1/kShards of the warps: room for its share of the list plus slack
     ps.shard_cap = capacity_ / kShards + 8192;
@@ -2421,7 +2330,7 @@ void Pool::launch_persistent(int n) {
     PoolState *ps = dstate_;
     void *args[] = {&ps, &n};
     CUDA_OK(cudaLaunchCooperativeKernel(kStepKernel[variant_].cycles, dim3(grid_cycles_[variant_]), dim3(kBlock), args,
-                                        kStepKernel[variant_].cycles_smem, st));
+                                        0, st));
     launches_ += 1;
 }
 
