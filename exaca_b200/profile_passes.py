@@ -5,6 +5,7 @@ prints their summed CUDA-event times. Under ncu this isolates one pass kernel on
 had time to form:
 
     python -m exaca_b200.profile_passes 256 --warm 3000 --cycles 3
+    python -m exaca_b200.profile_passes 288 --warm 4000 --launch 1000   # four k_cycles launches
     ncu --set full --clock-control none -k regex:k_grow -s 1 -c 1 -o prof_grow256 \\
         python -m exaca_b200.profile_passes 256 --warm 3000 --cycles 3
 """
@@ -21,6 +22,8 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("size", type=int, nargs="?", default=256, help="cube side in cells")
     ap.add_argument("--warm", type=int, default=3000, help="cycles in the persistent kernel first")
+    ap.add_argument("--launch", type=int, default=0,
+                    help="cycles per persistent launch of the warm-up (0: one launch), so a profiler can pick one")
     ap.add_argument("--cycles", type=int, default=3, help="cycles as separate pass kernels")
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args()
@@ -29,7 +32,13 @@ def main():
     pool = ex.Pool(args.device, list_capacity=prob.geometry.active_size)
     try:
         pool.admit(prob, device_check=False)
-        pool.step(args.warm)
+        if args.launch > 0:
+            done = 0
+            while done < args.warm:
+                pool.step(min(args.launch, args.warm - done))
+                done += args.launch
+        else:
+            pool.step(args.warm)
         passes = pool.profile_cycles(args.cycles)
         print(json.dumps({"size": n, "warm_cycles": args.warm, "pass_cycles": args.cycles,
                           "ms_per_pass": passes}), flush=True)
