@@ -58,14 +58,15 @@ PORT_LIB = os.path.join(ROOT, "oracle", "_port", "liboracle.so")
 #   grow/claim: record 16 + domain 4 + liquid mask 4 + growth-table entry 8 per listed record;
 #               diagonal/min-length write 8 per grown record; tombstone 16 + DiagonalLength 4 per
 #               dropped record; critical-length row 104 + min write 4 per flagged record; 26
-#               neighbour types + mask write 4 per fresh mask; 8 per claim; 8 per listed target
+#               neighbour types + mask write 4 per fresh mask; 8 per claim + its TemporaryUpdate
+#               CellType byte 1; 8 per listed target
 #   capture:    per capture: claim 8, target 8, GrainID 4+4, centres 12+12, orientation 36,
 #               DiagonalLength 4, 26 critical lengths 104, mask 4, record 16+4, CellType 1,
 #               CritTimeStep 4, and per neighbour direction CellType 1 + two mask atomics 8; per
 #               solidifying re-check CritTimeStep 4 + CellType 1 + mask 4
 PASS_BYTES = {
     "grow": dict(listed=24, grown=8, dropped=20, flagged=20),
-    "claim": dict(flagged=20 + 104 + 4, fresh=30, claims=8 + 8),
+    "claim": dict(flagged=20 + 104 + 4, fresh=30, claims=8 + 1 + 8),
     "capture": dict(claims=8 + 8, captured=221 + 26 * 9, rechecks=9),
 }
 

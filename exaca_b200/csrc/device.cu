@@ -786,7 +786,7 @@ __device__ __forceinline__ unsigned int claim_record(PoolState *P, ActiveRec *re
     if (m & kMaskFresh) {
         // liquid neighbours from the 26 neighbour types (src/CAupdate.cpp:320-334); no other thread
         // writes this cell's mask now, captures and nucleations clear bits later. Invalid directions
-        // read the cell itself.
+        // read the cell itself. A cell claimed in this same step (TemporaryUpdate) is still liquid.
         st.fresh++;
         int rx, ry, rz;
         cell_coords(D, c, rx, ry, rz);
@@ -797,7 +797,7 @@ __device__ __forceinline__ unsigned int claim_record(PoolState *P, ActiveRec *re
         for (int l = 0; l < 26; l++) {
             const bool v = (valid >> l) & 1u;
             const int8_t nt = __ldcg(ct + (v ? nb_offset(l, plane, my) : 0));
-            m |= (v && nt == kLiquid) ? (1u << l) : 0u;
+            m |= (v && (nt == kLiquid || nt == kTemporaryUpdate)) ? (1u << l) : 0u;
         }
         P->rstat[P->pending][i] = m;
     }
@@ -837,11 +837,16 @@ __device__ __forceinline__ unsigned int claim_record(PoolState *P, ActiveRec *re
     P->rmin2[P->pending][i] = ((unsigned long long)d1 << 32) | __float_as_uint(nm2);
     if (reach) {
         // claims (src/CAupdate.cpp:336-352): the lowest index wins. Nothing waits for them: every
-        // claimant lists its claim and the capture pass keeps the winner's.
+        // claimant lists its claim and the capture pass keeps the winner's. A claimed cell reads
+        // TemporaryUpdate until its capture makes it active, as in the reference's capture
+        // (src/CAupdate.cpp:343-352).
         const unsigned long long key = ((unsigned long long)(0xffffffffu - D.epoch) << 32) | (unsigned long long)c;
         unsigned long long *base = D.claim + c;
-        for (unsigned int bits = reach; bits; bits &= bits - 1)
-            atomicMin(base + nb_offset(__ffs(bits) - 1, plane, my), key);
+        for (unsigned int bits = reach; bits; bits &= bits - 1) {
+            const int nb = nb_offset(__ffs(bits) - 1, plane, my);
+            atomicMin(base + nb, key);
+            D.ctype[c + nb] = kTemporaryUpdate;
+        }
         st.claims += __popc(reach);
     }
     return reach;
@@ -1272,6 +1277,22 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
             continue;
         }
         const unsigned int w = c;
+        // The captured cell's liquid-neighbour mask, as its first claim step would build it from the
+        // neighbour types at the start of a later cycle: the neighbours still liquid (a neighbour
+        // claimed in this cycle reads TemporaryUpdate, or active once captured). Later captures and
+        // nucleations clear bits of it as of every other record's (it lies below later cycles' base).
+        unsigned int liq = 0;
+#pragma unroll
+        for (int k = 0; k < kPer; k++)
+            if (act[k] && ct[k] == kLiquid)
+                liq |= 1u << (sub + k * kCaptureLanes);
+        {
+            const unsigned int group = (kCaptureLanes == 32 ? 0xffffffffu : ((1u << kCaptureLanes) - 1u))
+                                       << (grp * kCaptureLanes);
+#pragma unroll
+            for (int o = kCaptureLanes / 2; o; o >>= 1)
+                liq |= __shfl_xor_sync(group, liq, o);
+        }
         // Serial order (src/CAupdate.cpp:333-334, 722-725): active cell a saw the captured cell t
         // as liquid iff t's capturer w does not precede a. a keeps a liquid neighbour iff it has an
         // unclaimed one (a set mask bit that nobody clears) or a claimed one with w >= a. Every
@@ -1302,7 +1323,7 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
             r.cts = cts_t;
             P->rec[app][base + j] = r;
             P->rdom[app][base + j] = dom;
-            rs[base + j] = kMaskFresh;
+            rs[base + j] = liq;
             P->rmin2[app][base + j] = kNoMin2;
             D.pos[t] = (unsigned int)(base + j);
             // read as active by the growth pass of the next cycle, after the octahedron is written
