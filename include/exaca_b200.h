@@ -255,7 +255,7 @@ typedef struct {
 /* Writes out[i] for domains[i], i < n_domains, equal to what exaca_pool_census reports for a slot
  * holding the same fields at the same cycle. `stream` is a cudaStream_t (NULL: the legacy default
  * stream); the call waits for it before returning. The first call on a device looks up the scratch
- * array's device address and loads the kernel; make that first call before any stream capture.
+ * array's device address and loads the kernel.
  * All calls on a device share the scratch array: a per-device lock keeps calls from several host
  * threads from overlapping on it. */
 int exaca_census_cells(int device, void *stream, const exaca_cell_fields *domains, int n_domains, exaca_census *out);
