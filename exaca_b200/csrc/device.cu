@@ -247,10 +247,12 @@ __device__ __forceinline__ long long domain_liquid(const DomainDesc &D) {
 // (src/CAupdate.cpp:353-563, 713-717).
 // Cooperative over kLanes lanes: every lane of the group evaluates the (identical) geometry, lane
 // `sub` computes critical lengths sub, sub + kLanes, ...; lane 0 of the group writes the scalar
-// state. Returns the new DiagonalLength.
+// state. Returns the new DiagonalLength. Over the directions in `liq` among the lane's own,
+// (mn, d1, mn2) receive the smallest critical length, its lowest direction and the second-smallest
+// (+inf and 0xffffffff where there is none), as a claim step's scan would find them.
 template <int kLanes>
 __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int t, int l, int sub, int h, float docx,
-                              float docy, float docz) {
+                              float docy, float docz, unsigned int liq, float &mn, unsigned int &d1, float &mn2) {
     int rx, ry, rz;
     cell_coords(D, c, rx, ry, rz);
     const int GlobalX = rx + D.xoff, GlobalY = ry + D.yoff, GlobalZ = rz;
@@ -362,7 +364,18 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
         double q2 = a0 * Fx[2] + b0 * Fy[2] + d0 * Fz[2];
         double q3 = a0 * Fx[3] + b0 * Fy[3] + d0 * Fz[3];
         double m = dmax(dmax(fabs(q0), fabs(q1)), dmax(fabs(q2), fabs(q3)));
-        D.cdl[26ull * t + n] = (float)m;
+        const float v = (float)m;
+        D.cdl[26ull * t + n] = v;
+        if ((liq >> n) & 1u) {
+            if (v < mn) {
+                mn2 = mn;
+                mn = v;
+                d1 = (unsigned int)n;
+            }
+            else if (v < mn2) {
+                mn2 = v;
+            }
+        }
     }
     return (float)NewODiagL;
 }
@@ -1314,17 +1327,40 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
             if (act[k])
                 old[k] = atomicAnd(rs + p[k], ~(1u << c_opp[sub + k * kCaptureLanes]));
         }
-        const float new_dl = capture_cell<kCaptureLanes>(D, c, t, l, sub, h, docx, docy, docz);
+        // The new record's cached minimum critical length over its liquid neighbours, with its
+        // direction and the second-smallest (the state a claim step leaves), so that its first claim
+        // step runs only once its DiagonalLength reaches a liquid neighbour.
+        float mn = __int_as_float(0x7f800000), mn2 = mn;
+        unsigned int d1 = 0xffffffffu;
+        const float new_dl =
+            capture_cell<kCaptureLanes>(D, c, t, l, sub, h, docx, docy, docz, liq, mn, d1, mn2);
+        {
+            const unsigned int group = (kCaptureLanes == 32 ? 0xffffffffu : ((1u << kCaptureLanes) - 1u))
+                                       << (grp * kCaptureLanes);
+#pragma unroll
+            for (int o = kCaptureLanes / 2; o; o >>= 1) {
+                const float omn = __shfl_xor_sync(group, mn, o), omn2 = __shfl_xor_sync(group, mn2, o);
+                const unsigned int od1 = __shfl_xor_sync(group, d1, o);
+                if (omn < mn || (omn == mn && od1 < d1)) {
+                    mn2 = fminf(omn2, mn);
+                    mn = omn;
+                    d1 = od1;
+                }
+                else {
+                    mn2 = fminf(mn2, omn);
+                }
+            }
+        }
         if (sub == 0) {
             ActiveRec r;
             r.cell = t;
             r.dl = new_dl;
-            r.cdl_min = 0.0f;
+            r.cdl_min = mn;
             r.cts = cts_t;
             P->rec[app][base + j] = r;
             P->rdom[app][base + j] = dom;
             rs[base + j] = liq;
-            P->rmin2[app][base + j] = kNoMin2;
+            P->rmin2[app][base + j] = ((unsigned long long)d1 << 32) | __float_as_uint(mn2);
             D.pos[t] = (unsigned int)(base + j);
             // read as active by the growth pass of the next cycle, after the octahedron is written
             D.ctype[t] = kActive;
