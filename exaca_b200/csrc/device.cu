@@ -787,15 +787,25 @@ __device__ __forceinline__ unsigned int claim_record(PoolState *P, ActiveRec *re
     const float dl = it.dl;
     DomainDesc &D = P->desc[dom];
     const int plane = D.mx * D.my, my = D.my;
-    // the 26 critical lengths as 13 aligned 8-byte loads (26 * 4 * c is 8-byte aligned)
-    const float2 *row = reinterpret_cast<const float2 *>(D.cdl + 26ull * c);
+    // the 26 critical lengths as 7 aligned 16-byte loads: a row (26 * 4 * c bytes in) starts on a
+    // 16-byte boundary for even c and 8 bytes past one for odd c, which read from 8 bytes before it
+    // (the previous row's end). The 8 bytes read past an even row lie in the array, or for the last
+    // row in the slot's next field array (sub-arrays start on 256-byte boundaries).
+    const bool odd = c & 1u;
+    const float4 *row = reinterpret_cast<const float4 *>(D.cdl + 26ull * c - (odd ? 2 : 0));
+    float f[28];
+#pragma unroll
+    for (int q = 0; q < 7; q++) {
+        const float4 v = __ldcg(row + q);
+        f[4 * q] = v.x;
+        f[4 * q + 1] = v.y;
+        f[4 * q + 2] = v.z;
+        f[4 * q + 3] = v.w;
+    }
     float cdl[26];
 #pragma unroll
-    for (int q = 0; q < 13; q++) {
-        const float2 v = __ldcg(row + q);
-        cdl[2 * q] = v.x;
-        cdl[2 * q + 1] = v.y;
-    }
+    for (int l = 0; l < 26; l++)
+        cdl[l] = odd ? f[l + 2] : f[l];
     if (m & kMaskFresh) {
         // liquid neighbours from the 26 neighbour types (src/CAupdate.cpp:320-334); no other thread
         // writes this cell's mask now, captures and nucleations clear bits later. Invalid directions
