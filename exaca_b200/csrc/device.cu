@@ -62,6 +62,10 @@ __constant__ unsigned int c_zminus;
 // direction index of a neighbour offset (dz+1)*9 + (dx+1)*3 + (dy+1), and opposite directions
 __constant__ int c_dir[27];
 __constant__ int c_opp[26];
+// The capture pass's order of neighbour slots, by z, then x, then y, so that consecutive slots are
+// neighbours in one row of three cells: slot s holds direction | opposite << 5 | ((dz + 1) |
+// (dx + 1) << 2 | (dy + 1) << 4) << 10, and 31 (no direction) for s >= 26.
+__constant__ unsigned int c_slot[32];
 
 constexpr unsigned int kMaskFresh = 1u << 31; // liquid-neighbour mask not built yet
 constexpr unsigned int kMaskDead = 1u << 30;  // solidified by a re-check: leaves the list next cycle
@@ -212,6 +216,10 @@ __device__ __forceinline__ unsigned int neighbour_mask(const DomainDesc &D, int 
 }
 
 __device__ __forceinline__ int nb_offset(int l, int plane, int my) { return c_nz[l] * plane + c_nx[l] * my + c_ny[l]; }
+// The same from the offset code (dz + 1) | (dx + 1) << 2 | (dy + 1) << 4 of a c_slot entry.
+__device__ __forceinline__ int code_offset(unsigned int code, int plane, int my) {
+    return ((int)(code & 3u) - 1) * plane + ((int)((code >> 2) & 3u) - 1) * my + ((int)((code >> 4) & 3u) - 1);
+}
 
 // Fresh octahedron of a newly active cell at its own centre (src/CAupdate.cpp:100-194,
 // src/CAinitialize.cpp:1942-2042): DL = 0.01, centre = cell centre, CDL from the orientation table.
@@ -1268,7 +1276,9 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         const int plane = D.mx * D.my, my = D.my;
         const unsigned int c = (unsigned int)((long long)t - nb_offset(l, plane, my)); // the claimant
         // Every load of the capture and of the re-checks goes out in one round; only the group of
-        // the winning claim (the lowest claimant index) continues.
+        // the winning claim (the lowest claimant index) continues. Lane `sub` takes the neighbour
+        // slots sub, sub + kCaptureLanes, ... (c_slot): a load instruction's lanes read neighbours
+        // in few rows of three consecutive cells.
         const unsigned long long key = __ldcg(D.claim + t);
         const int cts_t = __ldg(D.cts_run + t);
         const int h = __ldcg(D.gid + c);
@@ -1283,9 +1293,10 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         bool act[kPer];
 #pragma unroll
         for (int k = 0; k < kPer; k++) {
-            const int ln = sub + k * kCaptureLanes;
+            const unsigned int sc = c_slot[sub + k * kCaptureLanes];
+            const int ln = (int)(sc & 31u);
             act[k] = ln < 26 && (valid & (1u << ln));
-            a[k] = (unsigned int)((long long)t + (act[k] ? nb_offset(ln, plane, my) : 0));
+            a[k] = (unsigned int)((long long)t + (act[k] ? code_offset(sc >> 10, plane, my) : 0));
             ct[k] = __ldcg(D.ctype + a[k]);
             p[k] = __ldcg(D.pos + a[k]);
             cts_a[k] = __ldg(D.cts_run + a[k]);
@@ -1308,7 +1319,7 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
 #pragma unroll
         for (int k = 0; k < kPer; k++)
             if (act[k] && ct[k] == kLiquid)
-                liq |= 1u << (sub + k * kCaptureLanes);
+                liq |= 1u << (c_slot[sub + k * kCaptureLanes] & 31u);
         {
             const unsigned int group = (kCaptureLanes == 32 ? 0xffffffffu : ((1u << kCaptureLanes) - 1u))
                                        << (grp * kCaptureLanes);
@@ -1335,7 +1346,7 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         for (int k = 0; k < kPer; k++) {
             old[k] = 0;
             if (act[k])
-                old[k] = atomicAnd(rs + p[k], ~(1u << c_opp[sub + k * kCaptureLanes]));
+                old[k] = atomicAnd(rs + p[k], ~(1u << ((c_slot[sub + k * kCaptureLanes] >> 5) & 31u)));
         }
         // The new record's cached minimum critical length over its liquid neighbours, with its
         // direction and the second-smallest (the state a claim step leaves), so that its first claim
@@ -1382,7 +1393,7 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         for (int k = 0; k < kPer; k++) {
             if (!act[k])
                 continue;
-            const unsigned int bit = 1u << c_opp[sub + k * kCaptureLanes];
+            const unsigned int bit = 1u << ((c_slot[sub + k * kCaptureLanes] >> 5) & 31u);
             if ((old[k] & (kMaskFresh | kMaskDead)) || (old[k] & kDirBits) != bit || (old[k] & kMaskKeep))
                 continue;
             // a lost its last liquid neighbour; it solidifies if it was grown this cycle
@@ -1980,6 +1991,18 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
         opp[l] = dir[(1 - kNeighborZ[l]) * 9 + (1 - kNeighborX[l]) * 3 + (1 - kNeighborY[l])];
     CUDA_OK(cudaMemcpyToSymbol(c_dir, dir, sizeof(dir)));
     CUDA_OK(cudaMemcpyToSymbol(c_opp, opp, sizeof(opp)));
+    unsigned int slot[32];
+    int ns = 0;
+    for (int q = 0; q < 27; q++) // (dz, dx, dy) in row-major order
+        if (dir[q] >= 0) {
+            const int l = dir[q];
+            const unsigned int code = (unsigned int)((kNeighborZ[l] + 1) | (kNeighborX[l] + 1) << 2 |
+                                                     (kNeighborY[l] + 1) << 4);
+            slot[ns++] = (unsigned int)l | (unsigned int)opp[l] << 5 | code << 10;
+        }
+    for (; ns < 32; ns++)
+        slot[ns] = 31u;
+    CUDA_OK(cudaMemcpyToSymbol(c_slot, slot, sizeof(slot)));
     CUDA_OK(cudaMemcpyToSymbol(c_itmask, itmask, sizeof(itmask)));
     CUDA_OK(cudaMemcpyToSymbol(c_zplus, &zplus, sizeof(zplus)));
     CUDA_OK(cudaMemcpyToSymbol(c_zminus, &zminus, sizeof(zminus)));
