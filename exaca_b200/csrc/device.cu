@@ -2641,6 +2641,25 @@ void Pool::profile_persistent(int n, double us[7]) {
 }
 
 void Pool::set_config(int config) {
+    apply_config(config);
+    config_fixed_ = true;
+}
+
+void Pool::plain_tune(int n) {
+    int best = variant_;
+    double best_ms = 1e300;
+    for (int v = 0; v < kStepVariants; v++) {
+        apply_config(v);
+        const double ms = timed_step(n);
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = v;
+        }
+    }
+    apply_config(best);
+}
+
+void Pool::apply_config(int config) {
     if (config < 0 || config >= kStepConfigs)
         throw std::invalid_argument("step configuration out of range");
     const int mode = config / kStepVariants, variant = config % kStepVariants;
@@ -2657,7 +2676,7 @@ int Pool::autotune(int trial_cycles, double *ms_per_cycle) {
     int best = config();
     double best_ms = 1e300;
     for (int c = 0; c < kStepConfigs; c++) {
-        set_config(c);
+        apply_config(c);
         if (step_mode_ == 1)
             build_graph(); // outside the timed trial
         const double ms = timed_step(trial_cycles) / std::max(trial_cycles, 1);
@@ -2927,8 +2946,16 @@ int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_
     CUDA_OK(cudaEventRecord(ev0, S(stream_)));
     sync_state();
     int cycle = host_desc_[slot].cycle;
+    constexpr int kTuneCycles = 50;
     while (true) {
         int n = 1000 - (cycle % 1000);
+        if (!config_fixed_ && cycle % 4000 == 1000 && n == 1000) {
+            // the persistent configuration's speed depends on the domain's active front: time each
+            // for kTuneCycles real cycles at cycle 1000 and every 4000 cycles after; the results do
+            // not depend on it
+            plain_tune(kTuneCycles);
+            n -= kStepVariants * kTuneCycles;
+        }
         step(n);
         sync_state();
         const DomainDesc &d = host_desc_[slot];

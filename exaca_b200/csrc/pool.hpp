@@ -242,6 +242,8 @@ class Pool {
     // Step configurations: config = mode * kStepVariants + variant. set_config switches; autotune
     // runs trial_cycles real cycles with every configuration (the pool's domains advance), keeps
     // the fastest and returns it; ms_per_cycle (kStepConfigs entries, may be null) gets the trials.
+    // Either fixes the configuration for run_plain, which otherwise picks the fastest persistent
+    // one itself (plain_tune).
     static constexpr int kStepConfigs = 2 * kStepVariants;
     void set_config(int config);
     int config() const { return step_mode_ * kStepVariants + variant_; }
@@ -294,6 +296,10 @@ class Pool {
     // x launch-shape variant (kStepVariants compiled lane / batch combinations)
     int step_mode_ = 0;
     int variant_ = kStepVariants - 1;
+    bool config_fixed_ = false; // set_config or autotune chose the configuration
+    void apply_config(int config);
+    // run_plain's choice: n real cycles with each persistent configuration, the fastest kept
+    void plain_tune(int n);
     int grid_cycles_[kStepVariants] = {}; // co-resident blocks of each persistent kernel
     int grid_grow_[kStepVariants] = {};
     int grid_capture_[kStepVariants] = {};

@@ -133,7 +133,9 @@ int exaca_pool_step(exaca_pool *pool, int n_cycles);
 int exaca_pool_run_all(exaca_pool *pool, int chunk_cycles, int64_t max_cycles, int64_t *cycles_stepped);
 /* Step configurations (no counterpart in the reference): config = mode * 4 + shape, mode 0 the
  * persistent kernel and 1 a CUDA graph of the per-pass kernels, shape one of the compiled
- * {capture lanes 4|8} x {growth records per lane 2|4}. Results do not depend on the configuration. */
+ * {capture lanes 4|8} x {growth records per lane 2|4}. Results do not depend on the configuration.
+ * A configuration set here or chosen by exaca_pool_autotune stays; without either,
+ * exaca_pool_run_plain picks the fastest persistent one itself. */
 #define EXACA_STEP_CONFIGS 8
 int exaca_pool_set_config(exaca_pool *pool, int config);
 /* Autotuner: runs trial_cycles real cycles of the pool's domains in every configuration, keeps the
@@ -167,7 +169,8 @@ int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st);
 int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c);
 /* Runs one slot to completion exactly as the reference's layer loop (src/runCA.cpp:290-342):
  * 1000-cycle census, termination, type-S cycle jump; progress lines are appended to stdout when
- * verbose is 1. */
+ * verbose is 1. Unless a step configuration was set, it times the four persistent ones for 50 real
+ * cycles each at cycle 1000 of a layer and every 4000 cycles after, and keeps the fastest. */
 int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cycle);
 /* Ends the current layer of a multilayer slot and sets up the next: DomainShiftAndResize (the new
  * window from one plane below the lowest active cell to the highest cell of the next layer) and
