@@ -253,9 +253,12 @@ __device__ __forceinline__ long long domain_liquid(const DomainDesc &D) {
 // ---------------------------------------------------------------------------------------------
 // Capture of liquid cell t by active cell c through neighbour direction l
 // (src/CAupdate.cpp:353-563, 713-717).
-// Cooperative over kLanes lanes: every lane of the group evaluates the (identical) geometry, lane
-// `sub` computes critical lengths sub, sub + kLanes, ...; lane 0 of the group writes the scalar
-// state. Returns the new DiagonalLength. Over the directions in `liq` among the lane's own,
+// Cooperative over kLanes lanes: the group's lanes share the geometry, each independent division
+// and square root of a set (the three angles, normal components, distances and direction
+// components, the four side lengths, the two projections) evaluated once, on its own lane, with the
+// reference's expression, and passed to the others by shuffles; lane `sub` computes critical
+// lengths sub, sub + kLanes, ...; lane 0 of the group writes the scalar state. Returns the new
+// DiagonalLength. Over the directions in `liq` among the lane's own,
 // (mn, d1, mn2) receive the smallest critical length, its lowest direction and the second-smallest
 // (+inf and 0xffffffff where there is none), as a claim step's scan would find them.
 template <int kLanes>
@@ -278,13 +281,19 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     double x0 = xp - cxold;
     double y0 = yp - cyold;
     double z0 = zp - czold;
+    static_assert(kLanes >= 4 && kLanes <= 32, "the geometry spreads over at least four lanes");
+    const unsigned int gmask = (kLanes == 32 ? 0xffffffffu : ((1u << kLanes) - 1u))
+                               << ((int)(threadIdx.x & 31) / kLanes * kLanes);
     double mag0 = sqrtf((float)(x0 * x0 + y0 * y0 + z0 * z0));
-    double Angle1 = (g0 * x0 + g1 * y0 + g2 * z0) / mag0;
-    double Angle2 = (g3 * x0 + g4 * y0 + g5 * z0) / mag0;
-    double Angle3 = (g6 * x0 + g7 * y0 + g8 * z0) / mag0;
-    float s1 = (float)(2 * (Angle1 < 0) - 1);
-    float s2 = (float)(2 * (Angle2 < 0) - 1);
-    float s3 = (float)(2 * (Angle3 < 0) - 1);
+    // Angle1..3 on lanes 0..2 (src/CAupdate.cpp:379-381), their signs by ballot
+    const int q3 = sub < 3 ? sub : 0;
+    const float ga = q3 == 0 ? g0 : (q3 == 1 ? g3 : g6), gb = q3 == 0 ? g1 : (q3 == 1 ? g4 : g7),
+                gc = q3 == 0 ? g2 : (q3 == 1 ? g5 : g8);
+    double Angle = (ga * x0 + gb * y0 + gc * z0) / mag0;
+    const unsigned int neg = __ballot_sync(gmask, Angle < 0) >> ((int)(threadIdx.x & 31) / kLanes * kLanes);
+    float s1 = (float)(2 * (int)(neg & 1u) - 1);
+    float s2 = (float)(2 * (int)((neg >> 1) & 1u) - 1);
+    float s3 = (float)(2 * (int)((neg >> 2) & 1u) - 1);
     double Diag1X = g0 * s1, Diag1Y = g1 * s1, Diag1Z = g2 * s1;
     double Diag2X = g3 * s2, Diag2Y = g4 * s2, Diag2Z = g5 * s2;
     double Diag3X = g6 * s3, Diag3Y = g7 * s3, Diag3Z = g8 * s3;
@@ -294,7 +303,10 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     double UUy = U1z * U2x - U1x * U2z;
     double UUz = U1x * U2y - U1y * U2x;
     double NDem = sqrtf((float)(UUx * UUx + UUy * UUy + UUz * UUz));
-    double n0 = UUx / NDem, n1 = UUy / NDem, n2 = UUz / NDem;
+    // n0..n2 on lanes 0..2
+    const double nq = (q3 == 0 ? UUx : (q3 == 1 ? UUy : UUz)) / NDem;
+    double n0 = __shfl_sync(gmask, nq, 0, kLanes), n1 = __shfl_sync(gmask, nq, 1, kLanes),
+           n2 = __shfl_sync(gmask, nq, 2, kLanes);
     double ParaT = (n0 * x0 + n1 * y0 + n2 * z0) / (n0 * Diag1X + n1 * Diag1Y + n2 * Diag1Z);
     double TX[3], TY[3], TZ[3];
     TX[0] = cxold + ParaT * Diag1X;
@@ -306,11 +318,15 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     TX[2] = cxold + ParaT * Diag3X;
     TY[2] = cyold + ParaT * Diag3Y;
     TZ[2] = czold + ParaT * Diag3Z;
+    // Dist[0..2] on lanes 0..2
+    const double tqx = q3 == 0 ? TX[0] : (q3 == 1 ? TX[1] : TX[2]), tqy = q3 == 0 ? TY[0] : (q3 == 1 ? TY[1] : TY[2]),
+                 tqz = q3 == 0 ? TZ[0] : (q3 == 1 ? TZ[1] : TZ[2]);
+    const float distq =
+        sqrtf((float)(((tqx - xp) * (tqx - xp)) + ((tqy - yp) * (tqy - yp)) + ((tqz - zp) * (tqz - zp))));
     double Dist[3];
-#pragma unroll
-    for (int q = 0; q < 3; q++)
-        Dist[q] = sqrtf((float)(((TX[q] - xp) * (TX[q] - xp)) + ((TY[q] - yp) * (TY[q] - yp)) +
-                                ((TZ[q] - zp) * (TZ[q] - zp))));
+    Dist[0] = __shfl_sync(gmask, distq, 0, kLanes);
+    Dist[1] = __shfl_sync(gmask, distq, 1, kLanes);
+    Dist[2] = __shfl_sync(gmask, distq, 2, kLanes);
     int x = (Dist[0] < Dist[1]);
     int y = (Dist[1] < Dist[2]);
     int z = (Dist[2] < Dist[0]);
@@ -320,15 +336,25 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     int i1 = (idx + 1) % 3, i2 = (idx + 2) % 3;
     double x1 = TX[i1], y1 = TY[i1], z1 = TZ[i1];
     double x2 = TX[i2], y2 = TY[i2], z2 = TZ[i2];
-    double D1 = sqrtf((float)(((xp - x2) * (xp - x2)) + ((yp - y2) * (yp - y2)) + ((zp - z2) * (zp - z2))));
-    double D2 = sqrtf((float)(((xc - x2) * (xc - x2)) + ((yc - y2) * (yc - y2)) + ((zc - z2) * (zc - z2))));
-    double D3 = sqrtf((float)(((xp - x1) * (xp - x1)) + ((yp - y1) * (yp - y1)) + ((zp - z1) * (zp - z1))));
-    double D4 = sqrtf((float)(((xc - x1) * (xc - x1)) + ((yc - y1) * (yc - y1)) + ((zc - z1) * (zc - z1))));
+    // D1..D4 on lanes 0..3: D1 = |p - v2|, D2 = |c - v2|, D3 = |p - v1|, D4 = |c - v1|
+    const int q4 = sub & 3;
+    const double ax = (q4 & 1) ? xc : xp, ay = (q4 & 1) ? yc : yp, az = (q4 & 1) ? zc : zp;
+    const double bx = (q4 & 2) ? x1 : x2, by = (q4 & 2) ? y1 : y2, bz = (q4 & 2) ? z1 : z2;
+    const float dq = sqrtf((float)(((ax - bx) * (ax - bx)) + ((ay - by) * (ay - by)) + ((az - bz) * (az - bz))));
+    double D1 = __shfl_sync(gmask, dq, 0, kLanes);
+    double D2 = __shfl_sync(gmask, dq, 1, kLanes);
+    double D3 = __shfl_sync(gmask, dq, 2, kLanes);
+    double D4 = __shfl_sync(gmask, dq, 3, kLanes);
     double I1 = 0, I2 = D2, J1 = 0, J2 = D4;
     if (mindist != 0) {
-        I1 = D1 * ((xp - x2) * (xc - x2) + (yp - y2) * (yc - y2) + (zp - z2) * (zc - z2)) / (D1 * D2);
+        // I1 on lane 0, J1 on lane 1
+        const bool j = sub & 1;
+        const double ex = j ? x1 : x2, ey = j ? y1 : y2, ez = j ? z1 : z2;
+        const double Da = j ? D3 : D1, Db = j ? D4 : D2;
+        const double ij = Da * ((xp - ex) * (xc - ex) + (yp - ey) * (yc - ey) + (zp - ez) * (zc - ez)) / (Da * Db);
+        I1 = __shfl_sync(gmask, ij, 0, kLanes);
         I2 = D2 - I1;
-        J1 = D3 * ((xp - x1) * (xc - x1) + (yp - y1) * (yc - y1) + (zp - z1) * (zc - z1)) / (D3 * D4);
+        J1 = __shfl_sync(gmask, ij, 1, kLanes);
         J2 = D4 - J1;
     }
     const double sqrt3 = sqrt(3.0);
@@ -337,7 +363,10 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     double NewODiagL = sqrt(2.0) * dmax(L12, L13);
     double cd0 = xc - cxold, cd1 = yc - cyold, cd2 = zc - czold;
     double nd = sqrt(cd0 * cd0 + cd1 * cd1 + cd2 * cd2);
-    double uv0 = cd0 / nd, uv1 = cd1 / nd, uv2 = cd2 / nd;
+    // uv0..uv2 on lanes 0..2
+    const double uvq = (q3 == 0 ? cd0 : (q3 == 1 ? cd1 : cd2)) / nd;
+    double uv0 = __shfl_sync(gmask, uvq, 0, kLanes), uv1 = __shfl_sync(gmask, uvq, 1, kLanes),
+           uv2 = __shfl_sync(gmask, uvq, 2, kLanes);
     double cx = xc - NewODiagL * uv0;
     double cy = yc - NewODiagL * uv1;
     double cz = zc - NewODiagL * uv2;
