@@ -285,7 +285,7 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     const unsigned int gmask = (kLanes == 32 ? 0xffffffffu : ((1u << kLanes) - 1u))
                                << ((int)(threadIdx.x & 31) / kLanes * kLanes);
     double mag0 = sqrtf((float)(x0 * x0 + y0 * y0 + z0 * z0));
-    // Angle1..3 on lanes 0..2 (src/CAupdate.cpp:379-381), their signs by ballot
+    // Angle1..3 on lanes 0..2 (src/CAupdate.cpp:382-393), their signs by ballot
     const int q3 = sub < 3 ? sub : 0;
     const float ga = q3 == 0 ? g0 : (q3 == 1 ? g3 : g6), gb = q3 == 0 ? g1 : (q3 == 1 ? g4 : g7),
                 gc = q3 == 0 ? g2 : (q3 == 1 ? g5 : g8);
