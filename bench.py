@@ -63,11 +63,11 @@ PORT_LIB = os.path.join(ROOT, "oracle", "_port", "liboracle.so")
 #   capture:    per capture: claim 8, target 8, GrainID 4+4, centres 12+12, orientation 36,
 #               DiagonalLength 4, 26 critical lengths 104, mask 4, record 16+4, CellType 1,
 #               CritTimeStep 4, and per neighbour direction CellType 1 + two mask atomics 8; per
-#               solidifying re-check CritTimeStep 4 + CellType 1 + mask 4
+#               solidifying re-check CellType 1 + mask 4 (the mask word says whether it was grown)
 PASS_BYTES = {
     "grow": dict(listed=24, grown=8, dropped=20, flagged=20),
     "claim": dict(flagged=20 + 104 + 4, fresh=30, claims=8 + 1 + 8),
-    "capture": dict(claims=8 + 8, captured=221 + 26 * 9, rechecks=9),
+    "capture": dict(claims=8 + 8, captured=221 + 26 * 9, rechecks=5),
 }
 
 

@@ -70,6 +70,10 @@ __constant__ unsigned int c_slot[32];
 constexpr unsigned int kMaskFresh = 1u << 31; // liquid-neighbour mask not built yet
 constexpr unsigned int kMaskDead = 1u << 30;  // solidified by a re-check: leaves the list next cycle
 constexpr unsigned int kMaskKeep = 1u << 29;  // this cycle, a neighbour was captured by an index >= this cell's
+// the record has been grown (cycle > its CritTimeStep): set by the first growth step, so that the
+// capture pass's re-check needs no CritTimeStep (a record's eligibility only changes at a layer
+// change, which rebuilds the list)
+constexpr unsigned int kMaskGrown = 1u << 28;
 constexpr unsigned int kDirBits = (1u << 26) - 1;
 constexpr int kErrGrowthTable = 1;
 constexpr int kErrListOverflow = 2;
@@ -748,7 +752,7 @@ __device__ __forceinline__ int grow_record(DomainDesc &D, ActiveRec &r, unsigned
         st.flagged++;
         return 2;
     }
-    if (m == 0) {
+    if ((m & kDirBits) == 0) {
         // no liquid neighbour: LCount stays 0 (src/CAupdate.cpp:722-725)
         D.ctype[c] = kSolid;
         D.dl[c] = dl;
@@ -859,9 +863,9 @@ __device__ __forceinline__ unsigned int claim_record(PoolState *P, ActiveRec *re
             const int8_t nt = __ldcg(ct + (v ? nb_offset(l, plane, my) : 0));
             m |= (v && (nt == kLiquid || nt == kTemporaryUpdate)) ? (1u << l) : 0u;
         }
-        P->rstat[P->pending][i] = m;
+        P->rstat[P->pending][i] = m | kMaskGrown; // a flagged record was grown this cycle
     }
-    if (m == 0) {
+    if ((m & kDirBits) == 0) {
         // no liquid neighbour: LCount stays 0 (src/CAupdate.cpp:722-725)
         D.ctype[c] = kSolid;
         D.dl[c] = dl;
@@ -1082,7 +1086,10 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
                 double inc;
                 bool ok;
                 load_growth(desc[dom], r, inc, ok, extras);
-                keep = grow_record(desc[dom], r, m, inc, ok, effective_min(r, m, mn2), st) != 0;
+                const int a = grow_record(desc[dom], r, m, inc, ok, effective_min(r, m, mn2), st);
+                keep = a != 0;
+                if (a == 2)
+                    m |= kMaskGrown;
                 if (!keep)
                     st.dropped++;
             }
@@ -1191,6 +1198,10 @@ template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P,
             }
             else if (a == 2) {
                 *reinterpret_cast<float2 *>(&in[idx[q]].dl) = make_float2(r[q].dl, r[q].cdl_min);
+                if (!(m[q] & kMaskGrown)) {
+                    m[q] |= kMaskGrown;
+                    in_stat[idx[q]] = m[q];
+                }
                 if (__float_as_uint(r[q].cdl_min) == kNeedsClaim)
                     flagged |= 1u << q;
             }
@@ -1318,7 +1329,6 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         const unsigned int valid = neighbour_mask(D, tx, ty, tz);
         unsigned int a[kPer], p[kPer], old[kPer];
         int8_t ct[kPer];
-        int cts_a[kPer];
         bool act[kPer];
 #pragma unroll
         for (int k = 0; k < kPer; k++) {
@@ -1328,7 +1338,6 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
             a[k] = (unsigned int)((long long)t + (act[k] ? code_offset(sc >> 10, plane, my) : 0));
             ct[k] = __ldcg(D.ctype + a[k]);
             p[k] = __ldcg(D.pos + a[k]);
-            cts_a[k] = __ldg(D.cts_run + a[k]);
         }
         if ((unsigned int)key != c) {
             // a lower-index claimant captures t; this claim's slot stays a dropped record
@@ -1425,8 +1434,9 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
             const unsigned int bit = 1u << ((c_slot[sub + k * kCaptureLanes] >> 5) & 31u);
             if ((old[k] & (kMaskFresh | kMaskDead)) || (old[k] & kDirBits) != bit || (old[k] & kMaskKeep))
                 continue;
-            // a lost its last liquid neighbour; it solidifies if it was grown this cycle
-            if (D.cycle > cts_a[k]) {
+            // a lost its last liquid neighbour; it solidifies if it was grown this cycle (cycle >
+            // its CritTimeStep, src/CAupdate.cpp:257-261)
+            if (old[k] & kMaskGrown) {
                 st.rechecks++;
                 D.ctype[a[k]] = kSolid;
                 atomicOr(rs + p[k], kMaskDead);
