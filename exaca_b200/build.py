@@ -24,7 +24,7 @@ HOST_SOURCES = ["input.cpp", "init.cpp", "output.cpp", "capi.cpp", "rng.cpp"]
 # per-file optimisation level (the random-stream refill is vectorised at -O3)
 HOST_OPT = {"rng.cpp": "-O3"}
 CUDA_SOURCES = ["device.cu", "census_scratch.cu"]
-HEADERS = ["exaca_host.hpp", "pool.hpp", "rng.hpp"]
+HEADERS = ["exaca_host.hpp", "pool.hpp", "rng.hpp", "directions.hpp"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 GENCODE = ["-gencode", "arch=compute_100a,code=sm_100a"]
 CXX = "g++"

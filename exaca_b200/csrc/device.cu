@@ -51,21 +51,20 @@ namespace exaca {
             throw DeviceError(std::string("CUDA error ") + cudaGetErrorString(e__) + " at " #x);                     \
     } while (0)
 
-__constant__ int c_nx[26];
-__constant__ int c_ny[26];
-__constant__ int c_nz[26];
-// ItList (src/CAinitialize.cpp:676-745) as 26-bit direction masks per edge case, and the directions
-// with a z component of +1 / -1
-__constant__ unsigned int c_itmask[9];
-__constant__ unsigned int c_zplus;
-__constant__ unsigned int c_zminus;
-// direction index of a neighbour offset (dz+1)*9 + (dx+1)*3 + (dy+1), and opposite directions
-__constant__ int c_dir[27];
-__constant__ int c_opp[26];
-// The capture pass's order of neighbour slots, by z, then x, then y, so that consecutive slots are
-// neighbours in one row of three cells: slot s holds direction | opposite << 5 | ((dz + 1) |
-// (dx + 1) << 2 | (dy + 1) << 4) << 10, and 31 (no direction) for s >= 26.
-__constant__ unsigned int c_slot[32];
+// A direction's components, its opposite and the capture pass's slot order (directions.hpp), read
+// from immediates: lanes asking for different directions read no table.
+__device__ __forceinline__ int nb_dx(int l) { return (int)((kDirXP >> l) & 1u) - (int)((kDirXM >> l) & 1u); }
+__device__ __forceinline__ int nb_dy(int l) { return (int)((kDirYP >> l) & 1u) - (int)((kDirYM >> l) & 1u); }
+__device__ __forceinline__ int nb_dz(int l) { return (int)((kDirZP >> l) & 1u) - (int)((kDirZM >> l) & 1u); }
+__device__ __forceinline__ unsigned int field5(unsigned long long a, unsigned long long b, unsigned long long c,
+                                               int i) {
+    const unsigned long long v = i < 12 ? a : (i < 24 ? b : c);
+    const int f = i < 12 ? i : (i < 24 ? i - 12 : i - 24);
+    return (unsigned int)(v >> (5 * f)) & 31u;
+}
+__device__ __forceinline__ int nb_opp(int l) { return (int)field5(kOppA, kOppB, kOppC, l); }
+// direction of capture slot s (slots by z, then x, then y); 31 for s >= 26
+__device__ __forceinline__ int slot_dir(int s) { return s < 26 ? (int)field5(kSlotA, kSlotB, kSlotC, s) : 31; }
 
 constexpr unsigned int kMaskFresh = 1u << 31; // liquid-neighbour mask not built yet
 constexpr unsigned int kMaskDead = 1u << 30;  // solidified by a re-check: leaves the list next cycle
@@ -203,27 +202,26 @@ __device__ __forceinline__ void cell_coords(const DomainDesc &D, unsigned int c,
     ry = (int)(rem - x * (unsigned int)D.my);
 }
 
-// Edge case of src/CAfunctions.cpp:169-213 as a direction mask, restricted to the top of the active
-// window in z (src/CAupdate.cpp:328 checks MyNeighborZ < nzActive, window-relative; there is no
-// lower check in the reference, which reads one plane below the window; here z >= 0 is kept as a
-// guard).
-__device__ __forceinline__ unsigned int neighbour_mask(const DomainDesc &D, int rx, int ry, int rz) {
-    int b = (ry == 0) ? (rx == 0 ? 5 : (rx == D.mx - 1 ? 6 : 1))
-                      : (ry == D.my - 1 ? (rx == 0 ? 7 : (rx == D.mx - 1 ? 8 : 2))
-                                        : (rx == 0 ? 3 : (rx == D.mx - 1 ? 4 : 0)));
-    unsigned int m = c_itmask[b];
-    if (rz + 1 >= D.z_end)
-        m &= ~c_zplus;
+// Edge case of src/CAfunctions.cpp:169-213 as a direction mask (ItList, src/CAinitialize.cpp:676-745:
+// the edge cases drop the directions leaving the x / y extent, x = 0 before x = mx - 1 and y = 0
+// before y = my - 1), restricted to the top of the active window in z (src/CAupdate.cpp:328 checks
+// MyNeighborZ < nzActive, window-relative; there is no lower check in the reference, which reads
+// one plane below the window; here z >= 0 is kept as a guard).
+__device__ __forceinline__ unsigned int edge_mask(int rx, int ry, int rz, int mx, int my, int z_end) {
+    unsigned int m = (1u << 26) - 1u;
+    m &= ~(ry == 0 ? kDirYM : (ry == my - 1 ? kDirYP : 0u));
+    m &= ~(rx == 0 ? kDirXM : (rx == mx - 1 ? kDirXP : 0u));
+    if (rz + 1 >= z_end)
+        m &= ~kDirZP;
     if (rz - 1 < 0)
-        m &= ~c_zminus;
+        m &= ~kDirZM;
     return m;
 }
-
-__device__ __forceinline__ int nb_offset(int l, int plane, int my) { return c_nz[l] * plane + c_nx[l] * my + c_ny[l]; }
-// The same from the offset code (dz + 1) | (dx + 1) << 2 | (dy + 1) << 4 of a c_slot entry.
-__device__ __forceinline__ int code_offset(unsigned int code, int plane, int my) {
-    return ((int)(code & 3u) - 1) * plane + ((int)((code >> 2) & 3u) - 1) * my + ((int)((code >> 4) & 3u) - 1);
+__device__ __forceinline__ unsigned int neighbour_mask(const DomainDesc &D, int rx, int ry, int rz) {
+    return edge_mask(rx, ry, rz, D.mx, D.my, D.z_end);
 }
+
+__device__ __forceinline__ int nb_offset(int l, int plane, int my) { return nb_dz(l) * plane + nb_dx(l) * my + nb_dy(l); }
 
 // Fresh octahedron of a newly active cell at its own centre (src/CAupdate.cpp:100-194,
 // src/CAinitialize.cpp:1942-2042): DL = 0.01, centre = cell centre, CDL from the orientation table.
@@ -279,9 +277,9 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     const double cxold = docx;
     const double cyold = docy;
     const double czold = docz;
-    double xp = GlobalX + c_nx[l] + 0.5;
-    double yp = GlobalY + c_ny[l] + 0.5;
-    double zp = GlobalZ + c_nz[l] + 0.5;
+    double xp = GlobalX + nb_dx(l) + 0.5;
+    double yp = GlobalY + nb_dy(l) + 0.5;
+    double zp = GlobalZ + nb_dz(l) + 0.5;
     double x0 = xp - cxold;
     double y0 = yp - cyold;
     double z0 = zp - czold;
@@ -397,9 +395,9 @@ __device__ float capture_cell(const DomainDesc &D, unsigned int c, unsigned int 
     Fz[3] = g2 - g5 - g8;
 #pragma unroll 1
     for (int n = sub; n < 26; n += kLanes) {
-        double a0 = xp + c_nx[n] - cx;
-        double b0 = yp + c_ny[n] - cy;
-        double d0 = zp + c_nz[n] - cz;
+        double a0 = xp + nb_dx(n) - cx;
+        double b0 = yp + nb_dy(n) - cy;
+        double d0 = zp + nb_dz(n) - cz;
         double q0 = a0 * Fx[0] + b0 * Fy[0] + d0 * Fz[0];
         double q1 = a0 * Fx[1] + b0 * Fy[1] + d0 * Fz[1];
         double q2 = a0 * Fx[2] + b0 * Fy[2] + d0 * Fz[2];
@@ -587,14 +585,7 @@ __device__ __forceinline__ void start_domain(PoolState *P, DomainDesc &D, const 
             const unsigned int rem = site - z * (unsigned int)plane;
             const int rx = (int)(rem / (unsigned int)my), ry = (int)(rem - (unsigned int)rx * (unsigned int)my),
                       rz = (int)z;
-            const int b = (ry == 0) ? (rx == 0 ? 5 : (rx == mx - 1 ? 6 : 1))
-                                    : (ry == my - 1 ? (rx == 0 ? 7 : (rx == mx - 1 ? 8 : 2))
-                                                    : (rx == 0 ? 3 : (rx == mx - 1 ? 4 : 0)));
-            unsigned int valid = c_itmask[b];
-            if (rz + 1 >= z_end)
-                valid &= ~c_zplus;
-            if (rz - 1 < 0)
-                valid &= ~c_zminus;
+            const unsigned int valid = edge_mask(rx, ry, rz, mx, my, z_end);
             int ori = (abs(site_gid) - 1) % 10000;
             if (ori < 0)
                 ori += 10000;
@@ -634,7 +625,7 @@ __device__ __forceinline__ void start_domain(PoolState *P, DomainDesc &D, const 
                 s.ctype[site] = kActive;
             }
             if (nb && nb_type == kActive && nb_pos < cap)
-                atomicAnd(rstat + nb_pos, ~(1u << c_opp[lane]));
+                atomicAnd(rstat + nb_pos, ~(1u << nb_opp((int)lane)));
             __syncwarp();
         }
         fired_total += __popc(__ballot_sync(0xffffffffu, fire));
@@ -1317,8 +1308,8 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         const unsigned int c = (unsigned int)((long long)t - nb_offset(l, plane, my)); // the claimant
         // Every load of the capture and of the re-checks goes out in one round; only the group of
         // the winning claim (the lowest claimant index) continues. Lane `sub` takes the neighbour
-        // slots sub, sub + kCaptureLanes, ... (c_slot): a load instruction's lanes read neighbours
-        // in few rows of three consecutive cells.
+        // slots sub, sub + kCaptureLanes, ... (slot_dir): a load instruction's lanes read
+        // neighbours in few rows of three consecutive cells.
         const unsigned long long key = __ldcg(D.claim + t);
         const int cts_t = __ldg(D.cts_run + t);
         const int h = __ldcg(D.gid + c);
@@ -1332,10 +1323,9 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         bool act[kPer];
 #pragma unroll
         for (int k = 0; k < kPer; k++) {
-            const unsigned int sc = c_slot[sub + k * kCaptureLanes];
-            const int ln = (int)(sc & 31u);
+            const int ln = slot_dir(sub + k * kCaptureLanes);
             act[k] = ln < 26 && (valid & (1u << ln));
-            a[k] = (unsigned int)((long long)t + (act[k] ? code_offset(sc >> 10, plane, my) : 0));
+            a[k] = (unsigned int)((long long)t + (act[k] ? nb_offset(ln, plane, my) : 0));
             ct[k] = __ldcg(D.ctype + a[k]);
             p[k] = __ldcg(D.pos + a[k]);
         }
@@ -1357,7 +1347,7 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
 #pragma unroll
         for (int k = 0; k < kPer; k++)
             if (act[k] && ct[k] == kLiquid)
-                liq |= 1u << (c_slot[sub + k * kCaptureLanes] & 31u);
+                liq |= 1u << slot_dir(sub + k * kCaptureLanes);
         {
             const unsigned int group = (kCaptureLanes == 32 ? 0xffffffffu : ((1u << kCaptureLanes) - 1u))
                                        << (grp * kCaptureLanes);
@@ -1384,7 +1374,7 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         for (int k = 0; k < kPer; k++) {
             old[k] = 0;
             if (act[k])
-                old[k] = atomicAnd(rs + p[k], ~(1u << ((c_slot[sub + k * kCaptureLanes] >> 5) & 31u)));
+                old[k] = atomicAnd(rs + p[k], ~(1u << nb_opp(slot_dir(sub + k * kCaptureLanes))));
         }
         // The new record's cached minimum critical length over its liquid neighbours, with its
         // direction and the second-smallest (the state a claim step leaves), so that its first claim
@@ -1431,7 +1421,7 @@ template <int kCaptureLanes> __device__ void capture_pass(PoolState *P, CycleSta
         for (int k = 0; k < kPer; k++) {
             if (!act[k])
                 continue;
-            const unsigned int bit = 1u << ((c_slot[sub + k * kCaptureLanes] >> 5) & 31u);
+            const unsigned int bit = 1u << nb_opp(slot_dir(sub + k * kCaptureLanes));
             if ((old[k] & (kMaskFresh | kMaskDead)) || (old[k] & kDirBits) != bit || (old[k] & kMaskKeep))
                 continue;
             // a lost its last liquid neighbour; it solidifies if it was grown this cycle (cycle >
@@ -2004,47 +1994,24 @@ Pool::Pool(int device, size_t budget_bytes, unsigned long long list_capacity)
     cudaStream_t s;
     CUDA_OK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
     stream_ = s;
+    // the device's edge masks (edge_mask) are the reference's ItList cases
     int it[9][26], lens[9];
     build_itlist(it, lens);
-    CUDA_OK(cudaMemcpyToSymbol(c_nx, kNeighborX, sizeof(kNeighborX)));
-    CUDA_OK(cudaMemcpyToSymbol(c_ny, kNeighborY, sizeof(kNeighborY)));
-    CUDA_OK(cudaMemcpyToSymbol(c_nz, kNeighborZ, sizeof(kNeighborZ)));
-    unsigned int itmask[9], zplus = 0, zminus = 0;
     for (int b = 0; b < 9; b++) {
-        itmask[b] = 0;
+        unsigned int m = 0, want = (1u << 26) - 1u;
         for (int q = 0; q < lens[b]; q++)
-            itmask[b] |= 1u << it[b][q];
+            m |= 1u << it[b][q];
+        if (b == 1 || b == 5 || b == 6)
+            want &= ~kDirYM;
+        if (b == 2 || b == 7 || b == 8)
+            want &= ~kDirYP;
+        if (b == 3 || b == 5 || b == 7)
+            want &= ~kDirXM;
+        if (b == 4 || b == 6 || b == 8)
+            want &= ~kDirXP;
+        if (m != want)
+            throw std::logic_error("edge masks differ from ItList");
     }
-    for (int l = 0; l < 26; l++) {
-        if (kNeighborZ[l] == 1)
-            zplus |= 1u << l;
-        if (kNeighborZ[l] == -1)
-            zminus |= 1u << l;
-    }
-    int dir[27], opp[26];
-    for (int q = 0; q < 27; q++)
-        dir[q] = -1;
-    for (int l = 0; l < 26; l++)
-        dir[(kNeighborZ[l] + 1) * 9 + (kNeighborX[l] + 1) * 3 + (kNeighborY[l] + 1)] = l;
-    for (int l = 0; l < 26; l++)
-        opp[l] = dir[(1 - kNeighborZ[l]) * 9 + (1 - kNeighborX[l]) * 3 + (1 - kNeighborY[l])];
-    CUDA_OK(cudaMemcpyToSymbol(c_dir, dir, sizeof(dir)));
-    CUDA_OK(cudaMemcpyToSymbol(c_opp, opp, sizeof(opp)));
-    unsigned int slot[32];
-    int ns = 0;
-    for (int q = 0; q < 27; q++) // (dz, dx, dy) in row-major order
-        if (dir[q] >= 0) {
-            const int l = dir[q];
-            const unsigned int code = (unsigned int)((kNeighborZ[l] + 1) | (kNeighborX[l] + 1) << 2 |
-                                                     (kNeighborY[l] + 1) << 4);
-            slot[ns++] = (unsigned int)l | (unsigned int)opp[l] << 5 | code << 10;
-        }
-    for (; ns < 32; ns++)
-        slot[ns] = 31u;
-    CUDA_OK(cudaMemcpyToSymbol(c_slot, slot, sizeof(slot)));
-    CUDA_OK(cudaMemcpyToSymbol(c_itmask, itmask, sizeof(itmask)));
-    CUDA_OK(cudaMemcpyToSymbol(c_zplus, &zplus, sizeof(zplus)));
-    CUDA_OK(cudaMemcpyToSymbol(c_zminus, &zminus, sizeof(zminus)));
     max_domains_ = 8192;
     // list positions are 32-bit in the passes' block-local queues
     if (list_capacity > 0xffffffffull)

@@ -11,6 +11,7 @@
 #include <stdexcept>
 #include <string>
 #include <vector>
+#include "directions.hpp"
 
 namespace exaca {
 
@@ -175,10 +176,7 @@ struct RunTimes {
 };
 void write_log(const Problem &p, const std::string &fname, int cycle, const RunTimes &t, std::string &out);
 
-// neighbour offsets in the reference's order (src/CAinitialize.cpp:595-674)
-extern const int kNeighborX[26];
-extern const int kNeighborY[26];
-extern const int kNeighborZ[26];
+// neighbour offsets in the reference's order (kNeighborX / Y / Z) are in directions.hpp
 // ItList(9,26) and the per-case list lengths (src/CAinitialize.cpp:676-745)
 void build_itlist(int itlist[9][26], int lens[9]);
 inline int find_it_bounds(int rx, int ry, int mx, int my) {

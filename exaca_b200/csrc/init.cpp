@@ -25,10 +25,6 @@
 
 namespace exaca {
 
-const int kNeighborX[26] = {0, 1, -1, 0, 0, -1, 1, -1, 1, 0, 0, 1, -1, 1, -1, 1, -1, 0, 1, -1, 0, 0, 1, -1, 1, -1};
-const int kNeighborY[26] = {-1, -1, -1, -1, -1, -1, -1, -1, -1, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1, 1, 1, 1, 1, 1, 1};
-const int kNeighborZ[26] = {0, 0, 0, 1, -1, 1, 1, -1, -1, 1, -1, 1, 1, -1, -1, 0, 0, 0, 0, 0, 1, -1, 1, 1, -1, -1};
-
 void build_itlist(int it[9][26], int lens[9]) {
     // Case 0 keeps all 26; the others drop the neighbours that would leave the rank's x/y extent
     // (src/CAinitialize.cpp:676-745).
