@@ -754,9 +754,77 @@ __device__ __forceinline__ int grow_record(DomainDesc &D, ActiveRec &r, unsigned
     return 2;
 }
 
+// The descriptor fields a growth step reads for every record, in registers: for the pool's first
+// domain they are loaded once per growth pass, for the others per record.
+struct GrowView {
+    DomainDesc *D;
+    const double *growth;
+    long long e_cycle; // executed cycles up to the current one
+    int cycle, growth_len;
+    bool done, jumps, zero_du;
+};
+__device__ __forceinline__ GrowView grow_view(DomainDesc &D) {
+    GrowView v;
+    v.D = &D;
+    v.growth = D.growth;
+    v.cycle = D.cycle;
+    v.e_cycle = executed_upto(D, v.cycle);
+    v.growth_len = D.growth_len;
+    v.done = D.done != 0;
+    v.jumps = D.n_jumps > 0;
+    v.zero_du = D.zero_du != 0;
+    return v;
+}
+
+// grow_record with the per-record descriptor fields from a view
+__device__ __forceinline__ int grow_record(const GrowView &v, ActiveRec &r, unsigned int m, double inc, bool inc_ok,
+                                           float eff_min, CycleStats &st) {
+    const unsigned int c = r.cell;
+    st.listed++;
+    if (v.done || (m & kMaskDead)) {
+        if (v.D->dl)
+            v.D->dl[c] = r.dl;
+        return 0;
+    }
+    if (!(v.cycle > r.cts))
+        return 1;
+    st.grown++;
+    if (!inc_ok)
+        atomicOr(&v.D->error, kErrGrowthTable);
+    const float dl = (float)((double)r.dl + inc);
+    r.dl = dl;
+    if ((m & kMaskFresh) || dl >= eff_min) {
+        r.cdl_min = __uint_as_float(kNeedsClaim);
+        st.flagged++;
+        return 2;
+    }
+    if ((m & kDirBits) == 0) {
+        v.D->ctype[c] = kSolid;
+        v.D->dl[c] = dl;
+        return 0;
+    }
+    return 2;
+}
+
 __device__ __forceinline__ float effective_min(const ActiveRec &r, unsigned int m, unsigned long long min2) {
     const unsigned int d1 = (unsigned int)(min2 >> 32);
     return (d1 >= 26u || ((m >> d1) & 1u)) ? r.cdl_min : __uint_as_float((unsigned int)min2);
+}
+
+// load_growth with the per-record descriptor fields from a view
+__device__ __forceinline__ void load_growth(const GrowView &v, const ActiveRec &r, double &inc, bool &ok, bool extras) {
+    long long nu = v.e_cycle - (v.jumps ? executed_upto(*v.D, r.cts) : (r.cts <= 0 ? 0ll : (long long)r.cts));
+    const double *table = v.growth;
+    if (extras) {
+        if (v.D->nu_base)
+            nu += __ldg(v.D->nu_base + r.cell);
+        if (v.D->du_class)
+            table += (size_t)__ldg(v.D->du_class + r.cell) * (size_t)v.growth_len;
+    }
+    if (v.zero_du && v.D->du[r.cell] == 0.0f)
+        nu = 0;
+    ok = nu >= 0 && nu < v.growth_len;
+    inc = (ok && v.cycle > r.cts) ? __ldg(table + nu) : 0.0;
 }
 
 __device__ __forceinline__ void load_growth(const DomainDesc &D, const ActiveRec &r, double &inc, bool &ok,
@@ -1141,6 +1209,7 @@ template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P,
     const bool extras = P->extras;
     unsigned long long tombs = 0;
     const unsigned long long groups = (n + 31) / 32;
+    const GrowView v0 = grow_view(desc[0]);
     // records are updated in place; dropped ones become tombstones
     for (unsigned long long g0 = gw; g0 < groups; g0 += kBatch * nw) {
         ActiveRec r[kBatch];
@@ -1174,7 +1243,10 @@ template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P,
                     m[q] &= ~kMaskKeep;
                     in_stat[idx[q]] = m[q];
                 }
-                load_growth(desc[dom[q]], r[q], inc[q], ok[q], extras);
+                if (dom[q] == 0)
+                    load_growth(v0, r[q], inc[q], ok[q], extras);
+                else
+                    load_growth(grow_view(desc[dom[q]]), r[q], inc[q], ok[q], extras);
             }
         }
         unsigned int flagged = 0;
@@ -1182,7 +1254,9 @@ template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P,
         for (int q = 0; q < kBatch; q++) {
             if (r[q].cell == kTombstone)
                 continue;
-            const int a = grow_record(desc[dom[q]], r[q], m[q], inc[q], ok[q], effective_min(r[q], m[q], mn2[q]), st);
+            const int a = dom[q] == 0 ? grow_record(v0, r[q], m[q], inc[q], ok[q], effective_min(r[q], m[q], mn2[q]), st)
+                                      : grow_record(grow_view(desc[dom[q]]), r[q], m[q], inc[q], ok[q],
+                                                    effective_min(r[q], m[q], mn2[q]), st);
             if (a == 0) {
                 in[idx[q]].cell = kTombstone;
                 in[idx[q]].cdl_min = 0.0f;
