@@ -690,11 +690,12 @@ __global__ void k_step_begin(PoolState *P) { begin_cycle(P, false, P->desc, P->n
 //               re-check-solidified cells, solidification of cells whose liquid mask is empty. A
 //               record whose mask must still be built, or whose diagonal reached the cached minimum
 //               critical length, goes to the claim queue.
-//   claim       one queue entry per thread: the liquid mask from the 26 neighbour types, the
-//               critical-length row (13 aligned 8-byte loads) and the claims (src/CAupdate.cpp:
-//               320-352); every claim is listed.
+//   claim       one queue entry per thread: the liquid mask from the 26 neighbour types when it is
+//               not built yet (nucleated and new-layer cells), the critical-length row (7 aligned
+//               16-byte loads) and the claims (src/CAupdate.cpp:320-352); every claim is listed.
 //   capture     kCaptureLanes lanes per listed claim: the winner's group captures the cell
-//               (src/CAupdate.cpp:353-563) and re-checks the captured cell's active neighbours.
+//               (src/CAupdate.cpp:353-563), builds the new record's liquid mask and cached minimum
+//               critical length, and re-checks the captured cell's active neighbours.
 // They run as three kernels per cycle (k_grow, k_claim, k_capture_pass) or, for stretches of
 // cycles, inside the persistent cooperative kernel k_cycles with grid-wide barriers between them.
 constexpr unsigned int kNeedsClaim = 0xffffffffu; // NaN pattern in ActiveRec::cdl_min
