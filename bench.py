@@ -469,9 +469,9 @@ def b200_arm(args, rank, world, local):
                          "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "traffic_source": "not measured in this run: ncu DRAM bytes per cycle of a 1000-cycle "
                                            "k_cycles launch (profiles/traffic_per_launch.txt) x the cycles of "
-                                           "this launch; the 512^3 figure is from the kernel before captured "
-                                           "cells' masks were built in the capture pass (that change moved "
-                                           "0.3 % fewer DRAM bytes at 288^3)",
+                                           "this launch; the 512^3 figure is from an earlier kernel version "
+                                           "(the current one moves 32 % fewer DRAM bytes per cycle at 288^3, "
+                                           "profiles/k_cycles_dirsolid288_dram.md)",
                          "algorithmic_bytes_per_launch": launch_bytes, "launch_ms": launch_ms,
                          "sample": f"one launch over cycles {args.profile_at + 1}-{args.profile_at + args.profile_cycles}",
                          "pass_bytes_per_launch": pass_bytes,

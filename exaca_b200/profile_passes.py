@@ -6,6 +6,7 @@ had time to form:
 
     python -m exaca_b200.profile_passes 256 --warm 3000 --cycles 3
     python -m exaca_b200.profile_passes 288 --warm 4000 --launch 1000   # four k_cycles launches
+    python -m exaca_b200.profile_passes 288 --warm 4000 --launch 1000 --config 0   # 4 lanes, 2 records
     ncu --set full --clock-control none -k regex:k_grow -s 1 -c 1 -o prof_grow256 \\
         python -m exaca_b200.profile_passes 256 --warm 3000 --cycles 3
 """
@@ -26,11 +27,15 @@ def main():
                     help="cycles per persistent launch of the warm-up (0: one launch), so a profiler can pick one")
     ap.add_argument("--cycles", type=int, default=3, help="cycles as separate pass kernels")
     ap.add_argument("--device", type=int, default=0)
+    ap.add_argument("--config", type=int, default=-1,
+                    help="step configuration (exaca_pool_set_config; -1: the pool's default)")
     args = ap.parse_args()
     n = args.size
     prob = ex.Problem.directional(n, n, n, **WORKLOAD)
     pool = ex.Pool(args.device, list_capacity=prob.geometry.active_size)
     try:
+        if args.config >= 0:
+            pool.set_config(args.config)
         pool.admit(prob, device_check=False)
         if args.launch > 0:
             done = 0
