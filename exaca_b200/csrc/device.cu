@@ -2502,8 +2502,13 @@ void Pool::launch_persistent(int n) {
     CUDA_OK(cudaMemsetAsync((char *)dstate_ + offsetof(PoolState, bar_count), 0, 2 * sizeof(unsigned int), st));
     PoolState *ps = dstate_;
     void *args[] = {&ps, &n};
-    CUDA_OK(cudaLaunchCooperativeKernel(kStepKernel[variant_].cycles, dim3(grid_cycles_[variant_]), dim3(kBlock), args,
-                                        0, st));
+    // half the co-resident blocks for a short list (fewer arrivals at every grid-wide meeting;
+    // measured faster below ~1.3e5 records, slower from ~2.5e5)
+    constexpr unsigned long long kHalfGridRecords = 1ull << 17;
+    if (!grid_tuned_)
+        grid_div_ = (last_records_ > 0 && last_records_ < kHalfGridRecords) ? 2 : 1;
+    const int grid = std::max(1, grid_cycles_[variant_] / grid_div_);
+    CUDA_OK(cudaLaunchCooperativeKernel(kStepKernel[variant_].cycles, dim3(grid), dim3(kBlock), args, 0, st));
     launches_ += 1;
 }
 
@@ -2577,7 +2582,16 @@ void Pool::sync_state() {
     if (!host_desc_.empty())
         CUDA_OK(cudaMemcpyAsync(host_desc_.data(), ddesc_, sizeof(DomainDesc) * host_desc_.size(),
                                 cudaMemcpyDeviceToHost, st));
+    // the list counters (cnt[2], capacity, tombs, cur): the length of the list the next cycle reads
+    constexpr size_t kCnt = offsetof(PoolState, cnt), kEnd = offsetof(PoolState, cur) + sizeof(int);
+    unsigned char lists[kEnd - kCnt];
+    CUDA_OK(cudaMemcpyAsync(lists, (char *)dstate_ + kCnt, sizeof(lists), cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
+    unsigned long long cnt[2];
+    int cur;
+    std::memcpy(cnt, lists, sizeof(cnt));
+    std::memcpy(&cur, lists + (offsetof(PoolState, cur) - kCnt), sizeof(cur));
+    last_records_ = cnt[cur & 1];
 }
 
 int Pool::check_bounded_wait() {
@@ -2728,18 +2742,27 @@ void Pool::set_config(int config) {
     config_fixed_ = true;
 }
 
-void Pool::plain_tune(int n) {
-    int best = variant_;
+int Pool::plain_tune(int n) {
+    int best = variant_, best_div = 1;
     double best_ms = 1e300;
-    for (int v = 0; v < kStepVariants; v++) {
-        apply_config(v);
-        const double ms = timed_step(n);
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = v;
+    grid_tuned_ = true;
+    // the half grid only for lists that are not clearly long (it measured 25 % slower at ~1e6
+    // records, where its trials would cost more than they can find)
+    const int max_div = last_records_ < (1ull << 19) ? 2 : 1;
+    for (int div = 1; div <= max_div; div++)
+        for (int v = 0; v < kStepVariants; v++) {
+            apply_config(v);
+            grid_div_ = div;
+            const double ms = timed_step(n);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = v;
+                best_div = div;
+            }
         }
-    }
     apply_config(best);
+    grid_div_ = best_div;
+    return max_div * kStepVariants * n;
 }
 
 void Pool::apply_config(int config) {
@@ -3017,6 +3040,11 @@ void Pool::copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type) 
 
 int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_s) {
     TraceRange trace("exaca run_plain");
+    // the grid its trials choose holds for this run only
+    struct GridReset {
+        bool &tuned;
+        ~GridReset() { tuned = false; }
+    } grid_reset{grid_tuned_};
     // src/runCA.cpp:282-411: the layer loop, each layer's cycles until no liquid of the layer is left
     const Problem &p = *slots_.at(slot).problem;
     const bool type_r = p.cfg.simulation_type == "R";
@@ -3034,10 +3062,9 @@ int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_
         int n = 1000 - (cycle % 1000);
         if (!config_fixed_ && cycle % 4000 == 1000 && n == 1000) {
             // the persistent configuration's speed depends on the domain's active front: time each
-            // for kTuneCycles real cycles at cycle 1000 and every 4000 cycles after; the results do
-            // not depend on it
-            plain_tune(kTuneCycles);
-            n -= kStepVariants * kTuneCycles;
+            // launch shape with the full and the half grid for kTuneCycles real cycles at cycle 1000
+            // and every 4000 cycles after; the results do not depend on it
+            n -= plain_tune(kTuneCycles);
         }
         step(n);
         sync_state();

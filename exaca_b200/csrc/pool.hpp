@@ -297,9 +297,16 @@ class Pool {
     int step_mode_ = 0;
     int variant_ = kStepVariants - 1;
     bool config_fixed_ = false; // set_config or autotune chose the configuration
+    // Persistent grid: all co-resident blocks (grid_div_ 1) or half of them (2), which cuts the
+    // grid-wide meetings' cost when the list is short. run_plain's trials choose it; otherwise it
+    // follows the list length read at the last sync_state.
+    int grid_div_ = 1;
+    bool grid_tuned_ = false;
+    unsigned long long last_records_ = 0;
     void apply_config(int config);
-    // run_plain's choice: n real cycles with each persistent configuration, the fastest kept
-    void plain_tune(int n);
+    // run_plain's choice: n real cycles with each persistent configuration (and grid), the fastest
+    // kept; returns the cycles run
+    int plain_tune(int n);
     int grid_cycles_[kStepVariants] = {}; // co-resident blocks of each persistent kernel
     int grid_grow_[kStepVariants] = {};
     int grid_capture_[kStepVariants] = {};

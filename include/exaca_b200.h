@@ -169,8 +169,11 @@ int exaca_pool_stats(exaca_pool *pool, exaca_pool_stats_t *st);
 int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c);
 /* Runs one slot to completion exactly as the reference's layer loop (src/runCA.cpp:290-342):
  * 1000-cycle census, termination, type-S cycle jump; progress lines are appended to stdout when
- * verbose is 1. Unless a step configuration was set, it times the four persistent ones for 50 real
- * cycles each at cycle 1000 of a layer and every 4000 cycles after, and keeps the fastest. */
+ * verbose is 1. Unless a step configuration was set, it times the four persistent ones (with all
+ * and with half of the co-resident blocks, for active lists below 2^19 records) for 50 real cycles
+ * each at cycle 1000 of a layer and every 4000 cycles after, and keeps the fastest. Otherwise the
+ * persistent kernel runs half of the co-resident blocks while the active list read at the last
+ * status holds fewer than 2^17 records. */
 int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cycle);
 /* Ends the current layer of a multilayer slot and sets up the next: DomainShiftAndResize (the new
  * window from one plane below the lowest active cell to the highest cell of the next layer) and
