@@ -103,10 +103,11 @@ __device__ __forceinline__ long long executed_upto(const DomainDesc &D, long lon
 // overflow (the pool error flag is set).
 __device__ __forceinline__ unsigned long long block_reserve_on(unsigned long long *counter, unsigned long long cap,
                                                               int *error, unsigned int n) {
-    __shared__ unsigned int s_warp[kBlock / 32];
+    __shared__ unsigned int s_warp[32];
     __shared__ unsigned long long s_base;
     __shared__ int s_ok;
-    const unsigned int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    // the launch's own warp count (callers launch with different block sizes)
+    const unsigned int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, n_warps = blockDim.x >> 5;
     unsigned int incl = n;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -118,7 +119,7 @@ __device__ __forceinline__ unsigned long long block_reserve_on(unsigned long lon
         s_warp[warp] = incl;
     __syncthreads();
     if (warp == 0) {
-        unsigned int v = lane < kBlock / 32 ? s_warp[lane] : 0;
+        unsigned int v = lane < n_warps ? s_warp[lane] : 0;
         unsigned int inc2 = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -126,9 +127,9 @@ __device__ __forceinline__ unsigned long long block_reserve_on(unsigned long lon
             if (lane >= (unsigned)o)
                 inc2 += u;
         }
-        if (lane < kBlock / 32)
+        if (lane < n_warps)
             s_warp[lane] = inc2 - v;
-        unsigned int total = __shfl_sync(0xffffffffu, inc2, kBlock / 32 - 1);
+        unsigned int total = __shfl_sync(0xffffffffu, inc2, n_warps - 1);
         if (lane == 0) {
             unsigned long long b = total ? atomicAdd(counter, (unsigned long long)total) : 0ull;
             s_ok = (b + total <= cap);
@@ -167,7 +168,7 @@ __device__ __forceinline__ unsigned long long warp_reserve(unsigned long long *c
 
 // Block-level sum of per-thread statistics into one shard of the pool counters.
 __device__ __forceinline__ void block_stats(PoolState *P, unsigned long long a, unsigned long long b, int ia, int ib) {
-    __shared__ unsigned long long s_a[kBlock / 32], s_b[kBlock / 32];
+    __shared__ unsigned long long s_a[32], s_b[32];
     for (int o = 16; o; o >>= 1) {
         a += __shfl_down_sync(0xffffffffu, a, o);
         b += __shfl_down_sync(0xffffffffu, b, o);
