@@ -77,7 +77,10 @@ constexpr unsigned int kDirBits = (1u << 26) - 1;
 constexpr int kErrGrowthTable = 1;
 constexpr int kErrListOverflow = 2;
 constexpr int kErrBounds = 4;
-constexpr int kBlock = 256;
+// One 512-thread block per SM for the persistent kernel (16 warps per SM, 128 registers each): half
+// the blocks of two 256-thread ones, so half the arrivals at every grid-wide meeting, and a claim
+// step of up to 512 flagged records per block in one round.
+constexpr int kBlock = 512;
 // rmin2 of a record whose minimum direction is not known: the cached minimum alone applies
 constexpr unsigned long long kNoMin2 = 0xffffffffull << 32;
 
@@ -1010,7 +1013,7 @@ __device__ __forceinline__ void list_claims(PoolState *P, unsigned int shard, un
 // as soon as the block has grown its records (no grid-wide wait between growth and claims). A
 // block that flags more than kBlockQueue records in a cycle sends the rest to the global queue,
 // whose claim pass then runs after a grid-wide barrier (a flag tells every block).
-constexpr int kBlockQueue = 640;
+constexpr int kBlockQueue = 1280;
 struct BlockQueue {
     ClaimItem *items;    // kBlockQueue entries in shared memory
     unsigned int *count; // in shared memory; may exceed kBlockQueue (the excess went global)
@@ -1650,7 +1653,7 @@ template <class F> __device__ bool grid_meet(PoolState *P, int tag, F &&serial) 
 }
 
 // n_cycles complete CA cycles (start, grow/claim, capture) in one cooperative launch.
-template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 2) k_cycles(PoolState *P, int n_cycles) {
+template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 1) k_cycles(PoolState *P, int n_cycles) {
     CycleStats st;
     // with many domains, their per-cycle start (termination, nucleation) runs across the grid
     // (the descriptors and their number change only between launches)
