@@ -20,8 +20,8 @@
 namespace exaca {
 
 // One twist of the 312-word state and the tempering of all 312 new words into out; returns the
-// smallest of them. Compiled for AVX2 and for the baseline instruction set; the loader picks the
-// one the host supports.
+// smallest of them. Compiled for AVX-512, AVX2 and the baseline instruction set; the loader picks
+// the best one the host supports.
 uint64_t mt64_twist_temper(uint64_t *s, uint64_t *out);
 
 class Mt64 {
