@@ -140,6 +140,7 @@ SIGNATURES = {
     "exaca_pool_status_many": ([_P, _I, ctypes.POINTER(_I), ctypes.POINTER(DomainStatus)], _I),
     "exaca_pool_grain_stats": ([_P, _I, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(GrainStatsT)], _I),
     "exaca_pool_set_config": ([_P, _I], _I),
+    "exaca_pool_set_grid": ([_P, _I], _I),
     "exaca_pool_autotune": ([_P, _I, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_double)], _I),
     "exaca_problem_pin": ([_P], _I),
     "exaca_census_cells": ([_I, _P, ctypes.POINTER(CellFieldsT), _I, ctypes.POINTER(CensusT)], _I),
@@ -391,6 +392,10 @@ class Pool:
 
     def set_config(self, config: int) -> None:
         _check(load_library().exaca_pool_set_config(self._h, config))
+
+    def set_grid(self, divisor: int) -> None:
+        """Persistent kernel grid: 1 all co-resident blocks, 2 half of them, 0 the pool's own choice."""
+        _check(load_library().exaca_pool_set_grid(self._h, divisor))
 
     def autotune(self, trial_cycles: int = 100):
         """Times every step configuration on trial_cycles real cycles; keeps and returns the fastest

@@ -351,6 +351,12 @@ int exaca_pool_set_config(exaca_pool *pool, int config) {
     return guarded([&] { pool->pool->set_config(config); });
 }
 
+int exaca_pool_set_grid(exaca_pool *pool, int divisor) {
+    if (!pool || divisor < 0 || divisor > 2)
+        return fail(EXACA_ERR_ARG, "grid divisor must be 0, 1 or 2");
+    return guarded([&] { pool->pool->set_grid(divisor); });
+}
+
 int exaca_pool_autotune(exaca_pool *pool, int trial_cycles, int *config, double *ms_per_cycle) {
     if (!pool || trial_cycles <= 0)
         return fail(EXACA_ERR_ARG, "bad argument");

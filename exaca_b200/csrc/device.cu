@@ -2509,7 +2509,9 @@ void Pool::launch_persistent(int n) {
     // half the co-resident blocks for a short list (fewer arrivals at every grid-wide meeting;
     // measured faster below ~1.3e5 records, slower from ~2.5e5)
     constexpr unsigned long long kHalfGridRecords = 1ull << 17;
-    if (!grid_tuned_)
+    if (grid_fixed_)
+        grid_div_ = grid_fixed_;
+    else if (!grid_tuned_)
         grid_div_ = (last_records_ > 0 && last_records_ < kHalfGridRecords) ? 2 : 1;
     const int grid = std::max(1, grid_cycles_[variant_] / grid_div_);
     CUDA_OK(cudaLaunchCooperativeKernel(kStepKernel[variant_].cycles, dim3(grid), dim3(kBlock), args, 0, st));
@@ -2746,14 +2748,21 @@ void Pool::set_config(int config) {
     config_fixed_ = true;
 }
 
+void Pool::set_grid(int divisor) {
+    if (divisor < 0 || divisor > 2)
+        throw std::invalid_argument("grid divisor must be 0, 1 or 2");
+    grid_fixed_ = divisor;
+}
+
 int Pool::plain_tune(int n) {
     int best = variant_, best_div = 1;
     double best_ms = 1e300;
     grid_tuned_ = true;
     // the half grid only for lists that are not clearly long (it measured 25 % slower at ~1e6
     // records, where its trials would cost more than they can find)
-    const int max_div = last_records_ < (1ull << 19) ? 2 : 1;
-    for (int div = 1; div <= max_div; div++)
+    const int min_div = grid_fixed_ ? grid_fixed_ : 1;
+    const int max_div = grid_fixed_ ? grid_fixed_ : (last_records_ < (1ull << 19) ? 2 : 1);
+    for (int div = min_div; div <= max_div; div++)
         for (int v = 0; v < kStepVariants; v++) {
             apply_config(v);
             grid_div_ = div;
@@ -2766,7 +2775,7 @@ int Pool::plain_tune(int n) {
         }
     apply_config(best);
     grid_div_ = best_div;
-    return max_div * kStepVariants * n;
+    return (max_div - min_div + 1) * kStepVariants * n;
 }
 
 void Pool::apply_config(int config) {

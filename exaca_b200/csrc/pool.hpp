@@ -246,6 +246,9 @@ class Pool {
     // one itself (plain_tune).
     static constexpr int kStepConfigs = 2 * kStepVariants;
     void set_config(int config);
+    // Persistent grid: 0 chooses itself (run_plain's trials, else the list length), 1 all co-resident
+    // blocks, 2 half of them.
+    void set_grid(int divisor);
     int config() const { return step_mode_ * kStepVariants + variant_; }
     int autotune(int trial_cycles, double *ms_per_cycle);
     // Steps every admitted domain in chunks of `chunk` cycles until each one has ended on the device
@@ -302,6 +305,7 @@ class Pool {
     // follows the list length read at the last sync_state.
     int grid_div_ = 1;
     bool grid_tuned_ = false;
+    int grid_fixed_ = 0; // set_grid's divisor, 0 when the grid chooses itself
     unsigned long long last_records_ = 0;
     void apply_config(int config);
     // run_plain's choice: n real cycles with each persistent configuration (and grid), the fastest

@@ -138,6 +138,11 @@ int exaca_pool_run_all(exaca_pool *pool, int chunk_cycles, int64_t max_cycles, i
  * exaca_pool_run_plain picks the fastest persistent one itself. */
 #define EXACA_STEP_CONFIGS 8
 int exaca_pool_set_config(exaca_pool *pool, int config);
+/* Grid of the persistent kernel (no counterpart in the reference): divisor 1 runs all co-resident
+ * blocks, 2 half of them (cheaper grid-wide meetings for short active lists), 0 (the default) lets
+ * the pool choose (exaca_pool_run_plain's trials, else the active list's length at the last status
+ * read). Results do not depend on it. */
+int exaca_pool_set_grid(exaca_pool *pool, int divisor);
 /* Autotuner: runs trial_cycles real cycles of the pool's domains in every configuration, keeps the
  * fastest; ms_per_cycle (EXACA_STEP_CONFIGS entries, may be NULL) receives the trial times. */
 int exaca_pool_autotune(exaca_pool *pool, int trial_cycles, int *config, double *ms_per_cycle);

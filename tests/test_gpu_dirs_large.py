@@ -78,3 +78,29 @@ def test_full_solve_equals_restatement(lib, case, capfd):
         assert pool.status(slot).error == 0
     finally:
         pool.close()
+
+
+# (step configuration, grid divisor): the four persistent launch shapes on all co-resident blocks,
+# two of them on half the blocks, and the CUDA graph of the per-pass kernels; the plain driver's
+# own choice switches between these during a solve, so each must give the pinned result alone.
+SHAPES = [(0, 1), (1, 1), (2, 1), (3, 1), (0, 2), (3, 2), (4, 0)]
+
+
+@pytest.mark.parametrize("config,grid", SHAPES)
+def test_full_solve_every_shape(lib, config, grid, tmp_path):
+    pin = json.load(open(os.path.join(GOLDEN, "DirS256.json")))
+    fin = pin["final"]
+    inp = tmp_path / "input.txt"
+    inp.write_text("\n".join(pin["input"]) + "\n")
+    prob = ex.Problem.from_file(str(inp))
+    pool = ex.Pool(0, list_capacity=prob.geometry.active_size)
+    try:
+        pool.set_config(config)
+        pool.set_grid(grid)
+        slot = pool.admit(prob, device_check=False)
+        assert pool.run_plain(slot) == fin["cycle"]
+        gid, ct = pool.copy_out(slot)
+        assert digests(gid, ct) == {k: fin[k] for k in ("sha_grain_id", "sha_cell_type")}
+        assert pool.status(slot).error == 0
+    finally:
+        pool.close()
