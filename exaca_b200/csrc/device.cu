@@ -39,6 +39,7 @@
 #include <numeric>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 #include "pool.hpp"
 
@@ -2022,7 +2023,88 @@ template <class T> T *dalloc(size_t n, std::vector<void *> &allocs, size_t &byte
     bytes += b;
     return (T *)p;
 }
+
+// true when p is page-locked (or registered) host memory that a copy engine writes directly
+bool host_pinned(const void *p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Moves one staged piece into the caller's buffer on several host threads: len bytes, or with
+// widen len int8 values sign-extended to int32.
+void stage_move(char *dst, const char *src, size_t len, bool widen) {
+    constexpr size_t kPerThread = size_t(1) << 20;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nt = std::max<size_t>(1, std::min<size_t>({(size_t)hw, 8, len / kPerThread}));
+    auto part = [&](size_t t) {
+        const size_t lo = len * t / nt, hi = len * (t + 1) / nt;
+        if (widen) {
+            int32_t *o = (int32_t *)dst;
+            const int8_t *i = (const int8_t *)src;
+            for (size_t k = lo; k < hi; k++)
+                o[k] = i[k];
+        } else {
+            std::memcpy(dst + lo, src + lo, hi - lo);
+        }
+    };
+    std::vector<std::thread> workers;
+    for (size_t t = 1; t < nt; t++)
+        workers.emplace_back(part, t);
+    part(0);
+    for (auto &w : workers)
+        w.join();
+}
 } // namespace
+
+void Pool::to_host(const std::vector<HostCopy> &copies, void *stream) {
+    constexpr size_t kStageBytes = size_t(32) << 20;
+    cudaStream_t st = S(stream);
+    // page-locked destinations take their DMA as they are; the rest go through the staging pieces
+    struct Piece {
+        char *dst;
+        const char *src;
+        size_t len;
+        bool widen;
+    };
+    std::vector<Piece> pieces;
+    for (const HostCopy &c : copies) {
+        if (!c.dst || !c.bytes)
+            continue;
+        if (!c.widen && host_pinned(c.dst)) {
+            CUDA_OK(cudaMemcpyAsync(c.dst, c.src, c.bytes, cudaMemcpyDeviceToHost, st));
+            continue;
+        }
+        for (size_t off = 0; off < c.bytes; off += kStageBytes)
+            pieces.push_back({(char *)c.dst + (c.widen ? 4 * off : off), (const char *)c.src + off,
+                              std::min(kStageBytes, c.bytes - off), c.widen});
+    }
+    if (pieces.empty())
+        return;
+    if (!stage_[0]) {
+        for (int b = 0; b < 2; b++) {
+            CUDA_OK(cudaMallocHost(&stage_[b], kStageBytes));
+            cudaEvent_t e;
+            CUDA_OK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            stage_ev_[b] = e;
+        }
+    }
+    // two pieces in flight: the DMA of piece k+1 runs while the host threads move piece k out
+    auto issue = [&](size_t k) {
+        CUDA_OK(cudaMemcpyAsync(stage_[k & 1], pieces[k].src, pieces[k].len, cudaMemcpyDeviceToHost, st));
+        CUDA_OK(cudaEventRecord((cudaEvent_t)stage_ev_[k & 1], st));
+    };
+    issue(0);
+    for (size_t k = 0; k < pieces.size(); k++) {
+        if (k + 1 < pieces.size())
+            issue(k + 1);
+        CUDA_OK(cudaEventSynchronize((cudaEvent_t)stage_ev_[k & 1]));
+        stage_move(pieces[k].dst, (const char *)stage_[k & 1], pieces[k].len, pieces[k].widen);
+    }
+}
 
 void pin_problem(Problem &p) {
     auto reg = [](void *ptr, size_t bytes) {
@@ -2198,6 +2280,14 @@ Pool::~Pool() {
     }
     cudaFree(ddesc_);
     cudaFree(census_buf_);
+    if (copy_stream_)
+        cudaStreamSynchronize(S(copy_stream_));
+    for (int b = 0; b < 2; b++) {
+        if (stage_[b])
+            cudaFreeHost(stage_[b]);
+        if (stage_ev_[b])
+            cudaEventDestroy((cudaEvent_t)stage_ev_[b]);
+    }
     cudaStreamDestroy(S(stream_));
     if (copy_stream_)
         cudaStreamDestroy(S(copy_stream_));
@@ -2964,11 +3054,8 @@ void Pool::copy_out_raw(int slot, int32_t *grain_id, int8_t *cell_type) {
     const DomainDesc &d = host_desc_.at(slot);
     size_t N = slots_.at(slot).problem->g.domain_size;
     cudaStream_t st = S(stream_);
-    if (grain_id)
-        CUDA_OK(cudaMemcpyAsync(grain_id, d.gid, N * 4, cudaMemcpyDeviceToHost, st));
+    to_host({{grain_id, d.gid, N * 4, false}, {cell_type, d.ctype, N, false}}, stream_);
     d2h_bytes_ += (grain_id ? N * 4 : 0) + (cell_type ? N : 0);
-    if (cell_type)
-        CUDA_OK(cudaMemcpyAsync(cell_type, d.ctype, N, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
 }
 
@@ -2985,13 +3072,9 @@ void Pool::copy_octahedra(int slot, float *dl, float *doc, float *cdl) {
     // the current layer's window (the whole allocation's prefix for single-layer problems)
     const size_t plane = (size_t)d.mx * d.my, o = plane * d.z_lo, A = plane * (d.z_end - d.z_lo);
     cudaStream_t st = S(stream_);
-    if (dl)
-        CUDA_OK(cudaMemcpyAsync(dl, d.dl + o, A * 4, cudaMemcpyDeviceToHost, st));
+    to_host({{dl, d.dl + o, A * 4, false}, {doc, d.doc + 3 * o, A * 12, false}, {cdl, d.cdl + 26 * o, A * 104, false}},
+            stream_);
     d2h_bytes_ += (dl ? A * 4 : 0) + (doc ? A * 12 : 0) + (cdl ? A * 104 : 0);
-    if (doc)
-        CUDA_OK(cudaMemcpyAsync(doc, d.doc + 3 * o, A * 12, cudaMemcpyDeviceToHost, st));
-    if (cdl)
-        CUDA_OK(cudaMemcpyAsync(cdl, d.cdl + 26 * o, A * 104, cudaMemcpyDeviceToHost, st));
     CUDA_OK(cudaStreamSynchronize(st));
 }
 
@@ -3001,8 +3084,9 @@ void Pool::copy_out(int slot, int32_t *grain_id, int32_t *cell_type) {
         copy_out_raw(slot, grain_id, nullptr);
         return;
     }
-    // CellType is widened to int32 on the device (in stream order after the cycles), so both fields
-    // go straight into the caller's buffers (a DMA when they are pinned) with no host pass
+    // CellType is widened to int32 on the device (in stream order after the cycles); both fields
+    // then go to the caller's buffers as one DMA each when those are page-locked, else through the
+    // pinned staging pieces
     CUDA_OK(cudaSetDevice(device_));
     const DomainDesc &d = host_desc_.at(slot);
     const size_t N = slots_.at(slot).problem->g.domain_size;
@@ -3012,9 +3096,7 @@ void Pool::copy_out(int slot, int32_t *grain_id, int32_t *cell_type) {
     const unsigned blocks = (unsigned)std::min<size_t>((N + 255) / 256, (size_t)num_sms_ * 16);
     k_widen_types<<<blocks, 256, 0, st>>>(d.ctype, wide, (long long)N);
     CUDA_OK(cudaGetLastError());
-    if (grain_id)
-        CUDA_OK(cudaMemcpyAsync(grain_id, d.gid, N * 4, cudaMemcpyDeviceToHost, st));
-    CUDA_OK(cudaMemcpyAsync(cell_type, wide, N * 4, cudaMemcpyDeviceToHost, st));
+    to_host({{grain_id, d.gid, N * 4, false}, {cell_type, wide, N * 4, false}}, stream_);
     CUDA_OK(cudaFreeAsync(wide, st));
     CUDA_OK(cudaStreamSynchronize(st));
     d2h_bytes_ += (grain_id ? N * 4 : 0) + N * 4;
@@ -3035,20 +3117,12 @@ void Pool::copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type) 
     // The domain's GrainID and CellType are final (an ended domain's records only leave the list),
     // and the host saw that state, so the copies need no ordering against the pool stream. Copy
     // engines only: no kernel runs beside the persistent cooperative one.
+    // CellType is widened on the host as it leaves the staging pieces.
     cudaStream_t cs = S(copy_stream_);
     const size_t N = s.problem->g.domain_size;
-    std::vector<int8_t> ct;
-    if (grain_id)
-        CUDA_OK(cudaMemcpyAsync(grain_id, d.gid, N * 4, cudaMemcpyDeviceToHost, cs));
-    if (cell_type) {
-        ct.resize(N);
-        CUDA_OK(cudaMemcpyAsync(ct.data(), d.ctype, N, cudaMemcpyDeviceToHost, cs));
-    }
+    to_host({{grain_id, d.gid, N * 4, false}, {cell_type, d.ctype, N, true}}, copy_stream_);
     CUDA_OK(cudaStreamSynchronize(cs));
     d2h_bytes_ += (grain_id ? N * 4 : 0) + (cell_type ? N : 0);
-    if (cell_type)
-        for (size_t i = 0; i < N; i++)
-            cell_type[i] = ct[i];
 }
 
 int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_s) {

@@ -221,6 +221,20 @@ class Pool {
     // results while the next cycles run. Returns when the data is on the host.
     void copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type);
     void copy_octahedra(int slot, float *dl, float *doc, float *cdl);
+    // One device-to-host transfer of to_host: bytes from device memory src to host dst, or with
+    // widen bytes int8 values to int32 at dst. A null dst is skipped.
+    struct HostCopy {
+        void *dst;
+        const void *src;
+        size_t bytes;
+        bool widen;
+    };
+    // Issues the transfers on stream (a cudaStream_t) after the work already queued there and
+    // returns when every pageable destination holds its data; page-locked destinations take one
+    // DMA each, still in flight at return. Pageable ones go through two 32 MB pinned staging
+    // pieces, the DMA of one overlapping the multi-threaded move out of the other: the driver's
+    // own pageable path moves about 2 GB/s.
+    void to_host(const std::vector<HostCopy> &copies, void *stream);
     // writes the diagonal lengths held in the active records back to the per-cell array
     void flush_records();
     // Reference-equivalent run of one slot to completion with the reference's 1000-cycle census,
@@ -285,6 +299,8 @@ class Pool {
     size_t bytes_in_use_ = 0;
     void *stream_ = nullptr;      // cudaStream_t
     void *copy_stream_ = nullptr; // cudaStream_t of copy_out_concurrent (created on first use)
+    void *stage_[2] = {nullptr, nullptr};    // to_host's pinned staging pieces (first use)
+    void *stage_ev_[2] = {nullptr, nullptr}; // cudaEvent_t marking each piece's DMA
     PoolState *dstate_ = nullptr;
     DomainDesc *ddesc_ = nullptr;
     int max_domains_ = 0;

@@ -193,7 +193,8 @@ double exaca_pool_last_run_ms(exaca_pool *pool);
  * returns the summed times in kernel_ms[4] = {cycle start + nucleation, growth pass, claim pass,
  * capture + neighbour re-check pass}. */
 int exaca_pool_profile_cycles(exaca_pool *pool, int n_cycles, double *kernel_ms);
-/* Device->host copy of GrainID and CellType (src/runCA.cpp:423-424); NULL skips a field. */
+/* Device->host copy of GrainID and CellType (src/runCA.cpp:423-424); NULL skips a field. Page-locked
+ * buffers take one DMA per field; pageable ones go through the pool's pinned staging pieces. */
 int exaca_pool_copy_out(exaca_pool *pool, int slot, int32_t *grain_id, int32_t *cell_type);
 /* exaca_pool_copy_out for a slot whose domain has ended as of the last exaca_pool_status(_many) /
  * run_plain: the copies use the pool's separate copy stream and do not wait for cycles launched
