@@ -394,7 +394,7 @@ class Pool:
         _check(load_library().exaca_pool_set_config(self._h, config))
 
     def set_grid(self, divisor: int) -> None:
-        """Persistent kernel grid: 1 all co-resident blocks, 2 half of them, 0 the pool's own choice."""
+        """Persistent kernel grid: divisor d in 1-32 runs 1/d of the co-resident blocks, 0 the pool's own choice."""
         _check(load_library().exaca_pool_set_grid(self._h, divisor))
 
     def autotune(self, trial_cycles: int = 100):

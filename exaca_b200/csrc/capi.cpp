@@ -352,8 +352,8 @@ int exaca_pool_set_config(exaca_pool *pool, int config) {
 }
 
 int exaca_pool_set_grid(exaca_pool *pool, int divisor) {
-    if (!pool || divisor < 0 || divisor > 2)
-        return fail(EXACA_ERR_ARG, "grid divisor must be 0, 1 or 2");
+    if (!pool || divisor < 0 || divisor > 32)
+        return fail(EXACA_ERR_ARG, "grid divisor must be 0 (automatic) or 1-32");
     return guarded([&] { pool->pool->set_grid(divisor); });
 }
 

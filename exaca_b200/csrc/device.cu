@@ -2558,6 +2558,7 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     k_init_active<<<num_sms_ * 4, 256, 0, st>>>(dstate_, slot, -1);
     CUDA_OK(cudaGetLastError());
     bytes_in_use_ += s.bytes;
+    last_records_ = 0; // the list length is unknown until the next state read
     return slot;
 }
 
@@ -2596,13 +2597,14 @@ void Pool::launch_persistent(int n) {
     CUDA_OK(cudaMemsetAsync((char *)dstate_ + offsetof(PoolState, bar_count), 0, 2 * sizeof(unsigned int), st));
     PoolState *ps = dstate_;
     void *args[] = {&ps, &n};
-    // half the co-resident blocks for a short list (fewer arrivals at every grid-wide meeting;
-    // measured faster below ~1.3e5 records, slower from ~2.5e5)
-    constexpr unsigned long long kHalfGridRecords = 1ull << 17;
+    // a sixteenth of the co-resident blocks for a list too short to fill them (fewer arrivals at
+    // every grid-wide meeting; on a many-domain map measured faster below ~8e3 records, slower from
+    // ~1.7e4, and the half grid slower than the full one from ~3e4 up)
+    constexpr unsigned long long kSmallGridRecords = 1ull << 13;
     if (grid_fixed_)
         grid_div_ = grid_fixed_;
     else if (!grid_tuned_)
-        grid_div_ = (last_records_ > 0 && last_records_ < kHalfGridRecords) ? 2 : 1;
+        grid_div_ = (last_records_ > 0 && last_records_ < kSmallGridRecords) ? 16 : 1;
     const int grid = std::max(1, grid_cycles_[variant_] / grid_div_);
     CUDA_OK(cudaLaunchCooperativeKernel(kStepKernel[variant_].cycles, dim3(grid), dim3(kBlock), args, 0, st));
     launches_ += 1;
@@ -2839,8 +2841,8 @@ void Pool::set_config(int config) {
 }
 
 void Pool::set_grid(int divisor) {
-    if (divisor < 0 || divisor > 2)
-        throw std::invalid_argument("grid divisor must be 0, 1 or 2");
+    if (divisor < 0 || divisor > 32)
+        throw std::invalid_argument("grid divisor must be 0 (automatic) or 1-32");
     grid_fixed_ = divisor;
 }
 
@@ -3127,11 +3129,15 @@ void Pool::copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type) 
 
 int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_s) {
     TraceRange trace("exaca run_plain");
-    // the grid its trials choose holds for this run only
+    // the full grid until its trials choose, and the grid they choose holds for this run only (the
+    // short-list rule of chunked stepping would hold a small domain's first 1000 cycles, while its
+    // list grows from the initial front, on a sixteenth of the blocks)
     struct GridReset {
         bool &tuned;
         ~GridReset() { tuned = false; }
     } grid_reset{grid_tuned_};
+    grid_tuned_ = true;
+    grid_div_ = 1;
     // src/runCA.cpp:282-411: the layer loop, each layer's cycles until no liquid of the layer is left
     const Problem &p = *slots_.at(slot).problem;
     const bool type_r = p.cfg.simulation_type == "R";

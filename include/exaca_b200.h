@@ -138,8 +138,8 @@ int exaca_pool_run_all(exaca_pool *pool, int chunk_cycles, int64_t max_cycles, i
  * exaca_pool_run_plain picks the fastest persistent one itself. */
 #define EXACA_STEP_CONFIGS 8
 int exaca_pool_set_config(exaca_pool *pool, int config);
-/* Grid of the persistent kernel (no counterpart in the reference): divisor 1 runs all co-resident
- * blocks, 2 half of them (cheaper grid-wide meetings for short active lists), 0 (the default) lets
+/* Grid of the persistent kernel (no counterpart in the reference): divisor d in 1-32 runs 1/d of
+ * the co-resident blocks (cheaper grid-wide meetings for short active lists), 0 (the default) lets
  * the pool choose (exaca_pool_run_plain's trials, else the active list's length at the last status
  * read). Results do not depend on it. */
 int exaca_pool_set_grid(exaca_pool *pool, int divisor);
@@ -176,9 +176,9 @@ int exaca_pool_census(exaca_pool *pool, int slot, exaca_census *c);
  * 1000-cycle census, termination, type-S cycle jump; progress lines are appended to stdout when
  * verbose is 1. Unless a step configuration was set, it times the four persistent ones (with all
  * and with half of the co-resident blocks, for active lists below 2^19 records) for 50 real cycles
- * each at cycle 1000 of a layer and every 4000 cycles after, and keeps the fastest. Otherwise the
- * persistent kernel runs half of the co-resident blocks while the active list read at the last
- * status holds fewer than 2^17 records. */
+ * each at cycle 1000 of a layer and every 4000 cycles after, and keeps the fastest; before the first
+ * trials it runs all co-resident blocks. (exaca_pool_step and exaca_pool_run_all run a sixteenth of
+ * them while the active list read at the last status holds fewer than 2^13 records.) */
 int exaca_pool_run_plain(exaca_pool *pool, int slot, int verbose, int *final_cycle);
 /* Ends the current layer of a multilayer slot and sets up the next: DomainShiftAndResize (the new
  * window from one plane below the lowest active cell to the highest cell of the next layer) and

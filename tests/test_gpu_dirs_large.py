@@ -81,9 +81,10 @@ def test_full_solve_equals_restatement(lib, case, capfd):
 
 
 # (step configuration, grid divisor): the four persistent launch shapes on all co-resident blocks,
-# two of them on half the blocks, and the CUDA graph of the per-pass kernels; the plain driver's
-# own choice switches between these during a solve, so each must give the pinned result alone.
-SHAPES = [(0, 1), (1, 1), (2, 1), (3, 1), (0, 2), (3, 2), (4, 0)]
+# two of them on half the blocks, one on a sixteenth of them, and the CUDA graph of the per-pass
+# kernels; the drivers' own choices switch between these during a solve, so each must give the
+# pinned result alone.
+SHAPES = [(0, 1), (1, 1), (2, 1), (3, 1), (0, 2), (3, 2), (0, 16), (4, 0)]
 
 
 @pytest.mark.parametrize("config,grid", SHAPES)
