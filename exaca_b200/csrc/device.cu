@@ -507,7 +507,8 @@ __device__ __noinline__ void begin_lists(PoolState *P, bool close) { lists_start
 struct DomainStart {
     const int32_t *nuc_time, *nuc_loc;
     int8_t *ctype;
-    int done, check_mode, cycle0, cursor0, n_nuclei;
+    int done, check_mode, cycle0, cursor0, n_nuclei, dry_since;
+    bool drain; // a device-terminated domain whose cells are all past their CritTimeStep (every 64th cycle)
 };
 
 __device__ __forceinline__ DomainStart load_start(const DomainDesc &D) {
@@ -520,6 +521,8 @@ __device__ __forceinline__ DomainStart load_start(const DomainDesc &D) {
     s.done = __ldcg(&D.done);
     s.cycle0 = __ldcg(&D.cycle);
     s.cursor0 = __ldcg(&D.nuc_cursor);
+    s.dry_since = __ldcg(&D.dry_since);
+    s.drain = s.check_mode && (s.cycle0 & 63) == 0 && s.cycle0 - 2 >= D.cts_max;
     return s;
 }
 
@@ -549,6 +552,9 @@ __device__ __forceinline__ void start_domain(PoolState *P, DomainDesc &D, const 
     const unsigned int epoch0 = __ldcg(&D.epoch);
     const int nn0 = __ldcg(&D.nn);
     const long long liquid0 = __ldcg(&D.liquid);
+    // in the domain's last phase, every 64th cycle, whether any liquid is left (the shards load with
+    // this round; the answer is used after the sites, none of which can fire without liquid)
+    long long dry = s.drain && lane < kLiquidShards ? __ldcg(&D.liquid_shard[lane]) : 0;
     const unsigned long long cap = P->capacity;
     unsigned int *const rstat = P->rstat[cur];
     // src/CAupdate.cpp:76-198: sites with cycle >= NucleationTimes that are still liquid
@@ -640,7 +646,30 @@ __device__ __forceinline__ void start_domain(PoolState *P, DomainDesc &D, const 
         if (n_due < 32)
             break;
     }
-    if (lane == 0) {
+    bool ended = false;
+    if (s.drain) {
+#pragma unroll
+        for (int o = 16; o; o >>= 1)
+            dry += __shfl_xor_sync(0xffffffffu, dry, o);
+        if (dry + liquid0 == 0 && fired_total == 0) {
+            if (s.dry_since == 0) {
+                if (lane == 0)
+                    D.dry_since = s.cycle0;
+            }
+            else {
+                // At least a whole cycle has run with no liquid and every cell past its CritTimeStep,
+                // so every active cell has found no liquid neighbour and solidified
+                // (src/CAupdate.cpp:722-725); nothing changes until the next 1000-cycle check, which
+                // ends the domain (src/CAupdate.cpp:782-783). It ends here with that check's cycle.
+                ended = true;
+            }
+        }
+    }
+    if (lane == 0 && ended) {
+        D.cycle = (s.cycle0 + 999) / 1000 * 1000;
+        D.done = 1;
+    }
+    else if (lane == 0) {
         D.cycle = cycle;
         D.epoch = epoch0 + 1;
         D.nuc_cursor = cursor;
@@ -2507,11 +2536,13 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
     d.active_size = (long long)A;
     d.du_value = p.du_value;
     long long liquid = 0;
-    int zero_du = 0;
+    int zero_du = 0, cts_max = INT_MIN;
     if (p.dir.used) {
         // every cell inside the wall ring is liquid except the substrate seeds
         liquid = (long long)(g.mx - 2) * (g.my - 2) * (g.nz - 2) - (long long)p.dir.active.size();
         zero_du = p.du_value == 0.0f ? 1 : 0;
+        for (int32_t c : p.dir.plane_cts)
+            cts_max = std::max(cts_max, c);
     }
     else {
         for (long i = 0; i < g.domain_size; i++) {
@@ -2520,10 +2551,12 @@ int Pool::admit(std::shared_ptr<const Problem> pp, int check_mode) {
                 liquid++;
             if ((t == kLiquid || t == kActive) && p.du[i] == 0.0f)
                 zero_du = 1;
+            cts_max = std::max(cts_max, p.cts[i]);
         }
     }
     d.liquid = liquid;
     d.zero_du = zero_du;
+    d.cts_max = cts_max == INT_MIN ? INT_MAX : cts_max;
     host_desc_[slot] = d;
     push_desc(slot);
     if (multilayer) {

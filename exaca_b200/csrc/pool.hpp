@@ -84,6 +84,7 @@ struct DomainDesc {
     long long domain_size, active_size;
     float du_value;
     int zero_du; // 1 if a cell that can become active has UndercoolingChange 0 (U stays 0 there)
+    int cts_max; // check_mode domains: the largest CritTimeStep of any cell
     // dynamic state
     int cycle;
     unsigned int epoch;
@@ -92,6 +93,7 @@ struct DomainDesc {
     int nn;
     int error;
     int n_jumps;
+    int dry_since; // check_mode domains past cts_max: the first cycle start that found no liquid (0: none)
     long long liquid; // liquid cells of layer 0, less the nucleations (captures are in liquid_shard)
     long long liquid_shard[kLiquidShards]; // minus the captures, spread over shards to avoid contention
     int jump_lo[kMaxJumps];

@@ -121,7 +121,9 @@ int exaca_pool_create(int device, size_t budget_bytes, uint64_t list_capacity, e
 void exaca_pool_destroy(exaca_pool *pool);
 /* Uploads a problem (the host->device mirror copies of src/runCA.cpp:234-250) and finishes its
  * initialisation on the device. device_check = 1 lets the device end the domain at the
- * reference's termination test; 0 leaves it to exaca_pool_run_plain. */
+ * reference's termination test (at the 1000-cycle check that finds no liquid; once no liquid is
+ * left, every cell is past its CritTimeStep and at least one more cycle has run, the domain ends
+ * early with that check's cycle and the same fields); 0 leaves it to exaca_pool_run_plain. */
 int exaca_pool_admit(exaca_pool *pool, const exaca_problem *p, int device_check, int *slot);
 /* Advances every unfinished domain by n_cycles CA cycles: Nucleation + CellCapture
  * (src/CAupdate.hpp:15-29) per cycle, in one persistent kernel launch. Asynchronous. */
