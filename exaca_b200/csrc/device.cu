@@ -502,6 +502,16 @@ __device__ __forceinline__ void lists_start(PoolState *P, bool close, int *cur_o
 
 __device__ __noinline__ void begin_lists(PoolState *P, bool close) { lists_start(P, close, nullptr); }
 
+constexpr int kSerialDomains = 8; // up to this many domains one block starts each cycle alone
+
+// The domains that had not ended at the last state read, when there are at most kSerialDomains of
+// them (a kernel argument, so the cycle start reads their indices without a global round trip;
+// the first has the most cells). n < 0: start every domain of the pool.
+struct AliveSet {
+    int n;
+    int idx[kSerialDomains];
+};
+
 // Descriptor fields of the first round (the cursor into the nucleation sites and what decides
 // whether the domain runs this cycle).
 struct DomainStart {
@@ -696,18 +706,20 @@ __device__ __noinline__ void begin_domains(PoolState *P, DomainDesc *desc, int n
 // Cycle start by one block: the pool part in warp 0 while every warp loads its first domain's
 // descriptor, then the domains with the block's warps. With `close` it first ends the previous
 // cycle (finish_capture).
-__device__ __noinline__ void begin_cycle(PoolState *P, bool close, DomainDesc *desc, int n_domains) {
+__device__ __noinline__ void begin_cycle(PoolState *P, bool close, DomainDesc *desc, int n_domains, AliveSet alive) {
     __shared__ int s_cur;
     const int w = (int)(threadIdx.x >> 5), nw = (int)(blockDim.x >> 5);
+    const int n = alive.n < 0 ? n_domains : alive.n;
     DomainStart s{};
-    if (w < n_domains)
-        s = load_start(desc[w]);
+    if (w < n)
+        s = load_start(desc[alive.n < 0 ? w : alive.idx[w]]);
     lists_start(P, close, &s_cur);
     __syncthreads();
     const int cur = s_cur;
     unsigned long long nucleated = 0;
-    for (int d = w; d < n_domains; d += nw) {
-        if (d != w)
+    for (int i = w; i < n; i += nw) {
+        const int d = alive.n < 0 ? i : alive.idx[i];
+        if (i != w)
             s = load_start(desc[d]);
         start_domain(P, desc[d], s, (unsigned int)d, cur, nucleated);
     }
@@ -715,7 +727,7 @@ __device__ __noinline__ void begin_cycle(PoolState *P, bool close, DomainDesc *d
         atomicAdd(&P->stat[0][kStatNucleated], nucleated);
 }
 
-__global__ void k_step_begin(PoolState *P) { begin_cycle(P, false, P->desc, P->n_domains); }
+__global__ void k_step_begin(PoolState *P) { begin_cycle(P, false, P->desc, P->n_domains, AliveSet{-1, {}}); }
 
 // ---------------------------------------------------------------------------------------------
 // One CA cycle after its start (begin_cycle) is three passes over the pool:
@@ -1213,7 +1225,7 @@ __device__ __noinline__ void compact_pass(PoolState *P, int cur, unsigned long l
 // group g to warp g % (number of warps of the grid), consecutive warps on different blocks: the
 // records appended by the last capture pass, which all need a fresh mask and claims, spread over
 // every SM. No block-wide synchronisation.
-template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P, CycleStats &st) {
+template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P, CycleStats &st, unsigned int hot = 0) {
     const int cur = P->cur;
     const unsigned long long n = P->cnt[cur];
     const unsigned int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -1244,7 +1256,8 @@ template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P,
     const bool extras = P->extras;
     unsigned long long tombs = 0;
     const unsigned long long groups = (n + 31) / 32;
-    const GrowView v0 = grow_view(desc[0]);
+    // the growth fields of one domain (the one with the most cells among few) held in registers
+    const GrowView v0 = grow_view(desc[hot]);
     // records are updated in place; dropped ones become tombstones
     for (unsigned long long g0 = gw; g0 < groups; g0 += kBatch * nw) {
         ActiveRec r[kBatch];
@@ -1278,7 +1291,7 @@ template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P,
                     m[q] &= ~kMaskKeep;
                     in_stat[idx[q]] = m[q];
                 }
-                if (dom[q] == 0)
+                if (dom[q] == hot)
                     load_growth(v0, r[q], inc[q], ok[q], extras);
                 else
                     load_growth(grow_view(desc[dom[q]]), r[q], inc[q], ok[q], extras);
@@ -1289,7 +1302,7 @@ template <int kBatch, bool kBlockClaims> __device__ void grow_pass(PoolState *P,
         for (int q = 0; q < kBatch; q++) {
             if (r[q].cell == kTombstone)
                 continue;
-            const int a = dom[q] == 0 ? grow_record(v0, r[q], m[q], inc[q], ok[q], effective_min(r[q], m[q], mn2[q]), st)
+            const int a = dom[q] == hot ? grow_record(v0, r[q], m[q], inc[q], ok[q], effective_min(r[q], m[q], mn2[q]), st)
                                       : grow_record(grow_view(desc[dom[q]]), r[q], m[q], inc[q], ok[q],
                                                     effective_min(r[q], m[q], mn2[q]), st);
             if (a == 0) {
@@ -1599,7 +1612,7 @@ template <bool kBegin, int kLanes> __global__ void __launch_bounds__(kBlock) k_c
         if (threadIdx.x == 0)
             P->blocks_done = 0;
         if (kBegin)
-            begin_cycle(P, true, P->desc, P->n_domains);
+            begin_cycle(P, true, P->desc, P->n_domains, AliveSet{-1, {}});
         else
             finish_capture(P);
     }
@@ -1612,7 +1625,6 @@ template <bool kBegin, int kLanes> __global__ void __launch_bounds__(kBlock) k_c
 // wait is bounded: after kMeetTimeoutNs (or kMeetSpinCap polls) the block sets kErrBarrier and
 // the kernel ends.
 constexpr unsigned long long kMeetTimeoutNs = 1000000000ull;
-constexpr int kSerialDomains = 8; // up to this many domains one block starts each cycle alone
 constexpr unsigned int kMeetSpinCap = 1u << 26;
 
 __device__ __forceinline__ unsigned int ld_acquire_u32(const unsigned int *p) {
@@ -1683,19 +1695,22 @@ template <class F> __device__ bool grid_meet(PoolState *P, int tag, F &&serial) 
 }
 
 // n_cycles complete CA cycles (start, grow/claim, capture) in one cooperative launch.
-template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 1) k_cycles(PoolState *P, int n_cycles) {
+template <int kLanes, int kBatch>
+__global__ void __launch_bounds__(kBlock, 1) k_cycles(PoolState *P, int n_cycles, AliveSet alive) {
     CycleStats st;
-    // with many domains, their per-cycle start (termination, nucleation) runs across the grid
-    // (the descriptors and their number change only between launches)
+    // with many running domains, their per-cycle start (termination, nucleation) runs across the
+    // grid (the descriptors and their number change only between launches); with a few, one block
+    // starts them, and the first one's growth fields stay in registers
     DomainDesc *const desc = P->desc;
     const int n_domains = P->n_domains;
-    const bool spread = n_domains > kSerialDomains;
+    const bool spread = alive.n < 0 && n_domains > kSerialDomains;
+    const unsigned int hot = alive.n > 0 ? (unsigned int)alive.idx[0] : 0u;
     const int gwarp = (threadIdx.x >> 5) * gridDim.x + blockIdx.x, nwarp = gridDim.x * (kBlock / 32);
     bool ok = grid_meet(P, 0, [&] {
         if (spread)
             begin_lists(P, false);
         else
-            begin_cycle(P, false, desc, n_domains);
+            begin_cycle(P, false, desc, n_domains, alive);
     });
     if (ok && spread) {
         begin_domains(P, desc, n_domains, gwarp, nwarp);
@@ -1704,7 +1719,7 @@ template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 1) k
     for (int c = 0; ok && c < n_cycles; c++) {
         // growth with each block's claims right after its own growth; the global claim pass only
         // when some block's queue overflowed this cycle (the same answer for every block)
-        grow_pass<kBatch, true>(P, st);
+        grow_pass<kBatch, true>(P, st, hot);
         ok = grid_meet(P, 3 * c + 1, [] {});
         if (!ok)
             break;
@@ -1722,7 +1737,7 @@ template <int kLanes, int kBatch> __global__ void __launch_bounds__(kBlock, 1) k
             else if (spread)
                 begin_lists(P, true);
             else
-                begin_cycle(P, true, desc, n_domains);
+                begin_cycle(P, true, desc, n_domains, alive);
         });
         if (ok && more && spread) {
             begin_domains(P, desc, n_domains, gwarp, nwarp);
@@ -2629,7 +2644,22 @@ void Pool::launch_persistent(int n) {
     // the meeting point starts at zero arrivals (a launch that gave up waiting may have left some)
     CUDA_OK(cudaMemsetAsync((char *)dstate_ + offsetof(PoolState, bar_count), 0, 2 * sizeof(unsigned int), st));
     PoolState *ps = dstate_;
-    void *args[] = {&ps, &n};
+    // the domains still running at the last state read, when few (the one with most cells first);
+    // one that ends during the launch is still started and returns at once, as in the spread start
+    AliveSet alive{};
+    for (int s = 0; s < (int)slots_.size() && alive.n >= 0; s++) {
+        if (!slots_[s].used || host_desc_[s].done)
+            continue;
+        if (alive.n == kSerialDomains) {
+            alive.n = -1;
+            break;
+        }
+        alive.idx[alive.n++] = s;
+    }
+    for (int i = 1; i < alive.n; i++)
+        if (host_desc_[alive.idx[i]].active_size > host_desc_[alive.idx[0]].active_size)
+            std::swap(alive.idx[0], alive.idx[i]);
+    void *args[] = {&ps, &n, &alive};
     // a sixteenth of the co-resident blocks for a list too short to fill them (fewer arrivals at
     // every grid-wide meeting; on a many-domain map measured faster below ~8e3 records, slower from
     // ~1.7e4, and the half grid slower than the full one from ~3e4 up)
