@@ -517,8 +517,7 @@ struct AliveSet {
 struct DomainStart {
     const int32_t *nuc_time, *nuc_loc;
     int8_t *ctype;
-    int done, check_mode, cycle0, cursor0, n_nuclei, dry_since;
-    bool drain; // a device-terminated domain whose cells are all past their CritTimeStep (every 64th cycle)
+    int done, check_mode, cycle0, cursor0, n_nuclei;
 };
 
 __device__ __forceinline__ DomainStart load_start(const DomainDesc &D) {
@@ -531,8 +530,6 @@ __device__ __forceinline__ DomainStart load_start(const DomainDesc &D) {
     s.done = __ldcg(&D.done);
     s.cycle0 = __ldcg(&D.cycle);
     s.cursor0 = __ldcg(&D.nuc_cursor);
-    s.dry_since = __ldcg(&D.dry_since);
-    s.drain = s.check_mode && (s.cycle0 & 63) == 0 && s.cycle0 - 2 >= D.cts_max;
     return s;
 }
 
@@ -562,9 +559,13 @@ __device__ __forceinline__ void start_domain(PoolState *P, DomainDesc &D, const 
     const unsigned int epoch0 = __ldcg(&D.epoch);
     const int nn0 = __ldcg(&D.nn);
     const long long liquid0 = __ldcg(&D.liquid);
-    // in the domain's last phase, every 64th cycle, whether any liquid is left (the shards load with
-    // this round; the answer is used after the sites, none of which can fire without liquid)
-    long long dry = s.drain && lane < kLiquidShards ? __ldcg(&D.liquid_shard[lane]) : 0;
+    // every 64th cycle of a device-terminated domain, in its last phase (every cell past its
+    // CritTimeStep), whether any liquid is left: these loads go with this round, and the answer is
+    // used after the sites, none of which can fire without liquid
+    const bool probe = s.check_mode && (s.cycle0 & 63) == 0;
+    const int dry_since = probe ? __ldcg(&D.dry_since) : 0;
+    const int cts_max = probe ? D.cts_max : INT_MAX;
+    long long dry = probe && lane < kLiquidShards ? __ldcg(&D.liquid_shard[lane]) : 0;
     const unsigned long long cap = P->capacity;
     unsigned int *const rstat = P->rstat[cur];
     // src/CAupdate.cpp:76-198: sites with cycle >= NucleationTimes that are still liquid
@@ -657,12 +658,12 @@ __device__ __forceinline__ void start_domain(PoolState *P, DomainDesc &D, const 
             break;
     }
     bool ended = false;
-    if (s.drain) {
+    if (probe && s.cycle0 - 2 >= cts_max) {
 #pragma unroll
         for (int o = 16; o; o >>= 1)
             dry += __shfl_xor_sync(0xffffffffu, dry, o);
         if (dry + liquid0 == 0 && fired_total == 0) {
-            if (s.dry_since == 0) {
+            if (dry_since == 0) {
                 if (lane == 0)
                     D.dry_since = s.cycle0;
             }
@@ -2664,8 +2665,13 @@ void Pool::launch_persistent(int n) {
     // every grid-wide meeting; on a many-domain map measured faster below ~8e3 records, slower from
     // ~1.7e4, and the half grid slower than the full one from ~3e4 up)
     constexpr unsigned long long kSmallGridRecords = 1ull << 13;
+    // run_plain before its trials: half of them below 2^17 records (its first launch, while the
+    // list grows from the initial front)
+    constexpr unsigned long long kHalfGridRecords = 1ull << 17;
     if (grid_fixed_)
         grid_div_ = grid_fixed_;
+    else if (!grid_tuned_ && plain_run_)
+        grid_div_ = (last_records_ > 0 && last_records_ < kHalfGridRecords) ? 2 : 1;
     else if (!grid_tuned_)
         grid_div_ = (last_records_ > 0 && last_records_ < kSmallGridRecords) ? 16 : 1;
     const int grid = std::max(1, grid_cycles_[variant_] / grid_div_);
@@ -3192,15 +3198,14 @@ void Pool::copy_out_concurrent(int slot, int32_t *grain_id, int32_t *cell_type) 
 
 int Pool::run_plain(int slot, std::string &log, double *nucl_s, double *capture_s) {
     TraceRange trace("exaca run_plain");
-    // the full grid until its trials choose, and the grid they choose holds for this run only (the
-    // short-list rule of chunked stepping would hold a small domain's first 1000 cycles, while its
-    // list grows from the initial front, on a sixteenth of the blocks)
+    // its own grid rule until its trials choose, and the grid they choose holds for this run only
+    // (the short-list rule of chunked stepping would hold a small domain's first 1000 cycles, while
+    // its list grows from the initial front, on a sixteenth of the blocks)
     struct GridReset {
-        bool &tuned;
-        ~GridReset() { tuned = false; }
-    } grid_reset{grid_tuned_};
-    grid_tuned_ = true;
-    grid_div_ = 1;
+        bool &tuned, &plain;
+        ~GridReset() { tuned = plain = false; }
+    } grid_reset{grid_tuned_, plain_run_};
+    plain_run_ = true;
     // src/runCA.cpp:282-411: the layer loop, each layer's cycles until no liquid of the layer is left
     const Problem &p = *slots_.at(slot).problem;
     const bool type_r = p.cfg.simulation_type == "R";

@@ -323,6 +323,7 @@ class Pool {
     // follows the list length read at the last sync_state.
     int grid_div_ = 1;
     bool grid_tuned_ = false;
+    bool plain_run_ = false; // inside run_plain
     int grid_fixed_ = 0; // set_grid's divisor, 0 when the grid chooses itself
     unsigned long long last_records_ = 0;
     void apply_config(int config);
